@@ -1,0 +1,258 @@
+"""ctypes bindings of the CPU checkers -- TEST INFRASTRUCTURE ONLY.
+
+* ``liboracle.so``: the plain-C restatement of GANIT's restarted PDHG
+  (pdhg_oracle.c / pdhg_phase.inc; reference src/pdhg_impl.hpp,
+  src/backend_cpu.cpp, src/scaling.cpp).
+* ``_ref/libganit_ref.so``: the reference's own CPU implementation compiled
+  from its sources (see Makefile) behind ref_shim.cpp.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline / reference
+legs import this module.  The product package never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libganit_ref.so")
+
+STATUS = {0: "OPTIMAL", 1: "PRIMAL_INFEASIBLE", 2: "ITERATION_LIMIT", 3: "TIME_LIMIT", 4: "NUMERICAL_ERROR"}
+PRECISION = {"double": 0, "mixed": 1, "dynamic": 2}
+
+
+class _Lp(C.Structure):
+    _fields_ = [("m", C.c_int), ("n", C.c_int), ("a_ptr", C.c_void_p), ("a_idx", C.c_void_p),
+                ("a_val", C.c_void_p), ("c", C.c_void_p), ("l", C.c_void_p), ("u", C.c_void_p),
+                ("lo", C.c_void_p), ("hi", C.c_void_p), ("obj_const", C.c_double), ("maximize", C.c_int),
+                ("q_ptr", C.c_void_p), ("q_idx", C.c_void_p), ("q_val", C.c_void_p)]
+
+
+class _Opt(C.Structure):
+    _fields_ = [("tol", C.c_double), ("max_iter", C.c_long), ("time_limit", C.c_double),
+                ("check_every", C.c_int), ("ruiz_iters", C.c_int), ("pock_chambolle", C.c_int),
+                ("infeas_tol", C.c_double), ("precision", C.c_int), ("stall_checks", C.c_int),
+                ("stall_checks_l2", C.c_int)]
+
+
+class _OraRes(C.Structure):
+    _fields_ = [("status", C.c_int), ("pobj", C.c_double), ("dobj", C.c_double), ("rel_p", C.c_double),
+                ("rel_d", C.c_double), ("rel_gap", C.c_double), ("iterations", C.c_long),
+                ("fp32_iterations", C.c_long), ("l2_iterations", C.c_long), ("restarts", C.c_int),
+                ("setup_s", C.c_double), ("solve_s", C.c_double), ("norm_a", C.c_double),
+                ("w_final", C.c_double)]
+
+
+class _RefRes(C.Structure):
+    _fields_ = [("status", C.c_int), ("pobj", C.c_double), ("dobj", C.c_double), ("rel_p", C.c_double),
+                ("rel_d", C.c_double), ("rel_gap", C.c_double), ("iterations", C.c_long),
+                ("fp32_iterations", C.c_long), ("l2_iterations", C.c_long), ("restarts", C.c_int),
+                ("setup_s", C.c_double), ("solve_s", C.c_double)]
+
+
+@dataclass
+class OracleResult:
+    status: str
+    pobj: float
+    dobj: float
+    rel_p: float
+    rel_d: float
+    rel_gap: float
+    iterations: int
+    fp32_iterations: int
+    l2_iterations: int
+    restarts: int
+    setup_s: float
+    solve_s: float
+    x: np.ndarray
+    y: np.ndarray
+    norm_a: float = float("nan")
+
+
+def build(ref: bool = True) -> None:
+    """Compile the checkers with oracle/Makefile (the reference build only
+    when its sources are present on this machine)."""
+    targets = ["oracle"]
+    if ref and os.path.isdir("/root/reference/src"):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+_libs: dict = {}
+
+
+def _load(path: str):
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (run `make -C oracle`)")
+        _libs[path] = C.CDLL(path)
+    return _libs[path]
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def _options(precision="double", tol=1e-4, max_iter=10_000_000, time_limit=3600.0, check_every=64,
+             ruiz_iters=10, pock_chambolle=True, infeas_tol=1e-8, stall_checks=12, stall_checks_l2=24):
+    return _Opt(tol, max_iter, time_limit, check_every, ruiz_iters, int(pock_chambolle), infeas_tol,
+                PRECISION[precision] if isinstance(precision, str) else int(precision), stall_checks,
+                stall_checks_l2)
+
+
+def _arrays(lp):
+    if lp.F is not None:
+        raise ValueError("the oracle takes the reference's CSR Hessian; use the lifted QP form")
+    arrs = dict(ptr=lp.A.ptr, idx=lp.A.idx, val=lp.A.val, c=lp.c, l=lp.l, u=lp.u, lo=lp.lo, hi=lp.hi)
+    if lp.Q is not None and lp.Q.nnz:
+        arrs.update(qptr=lp.Q.ptr, qidx=lp.Q.idx, qval=lp.Q.val)
+    else:
+        arrs.update(qptr=None, qidx=None, qval=None)
+    return arrs
+
+
+def solve(lp, **opts) -> OracleResult:
+    """Run the C restatement (single thread)."""
+    lib = _load(ORACLE_SO)
+    a = _arrays(lp)
+    s = _Lp(lp.m, lp.n, _p(a["ptr"]), _p(a["idx"]), _p(a["val"]), _p(a["c"]), _p(a["l"]), _p(a["u"]),
+            _p(a["lo"]), _p(a["hi"]), float(lp.obj_const), int(lp.maximize), _p(a["qptr"]), _p(a["qidx"]),
+            _p(a["qval"]))
+    o = _options(**opts)
+    r = _OraRes()
+    x = np.zeros(lp.n)
+    y = np.zeros(lp.m)
+    lib.ora_solve_pdhg.restype = C.c_int
+    rc = lib.ora_solve_pdhg(C.byref(s), C.byref(o), C.byref(r), _p(x), _p(y))
+    if rc != 0:
+        raise RuntimeError(f"ora_solve_pdhg failed ({rc})")
+    return OracleResult(STATUS[r.status], r.pobj, r.dobj, r.rel_p, r.rel_d, r.rel_gap, r.iterations,
+                        r.fp32_iterations, r.l2_iterations, r.restarts, r.setup_s, r.solve_s, x, y, r.norm_a)
+
+
+def scale(lp, ruiz_iters=10, pock_chambolle=True) -> dict:
+    """Scaled data of src/scaling.cpp:36-155 (see ora_scale)."""
+    lib = _load(ORACLE_SO)
+    a = _arrays(lp)
+    s = _Lp(lp.m, lp.n, _p(a["ptr"]), _p(a["idx"]), _p(a["val"]), _p(a["c"]), _p(a["l"]), _p(a["u"]),
+            _p(a["lo"]), _p(a["hi"]), float(lp.obj_const), int(lp.maximize), _p(a["qptr"]), _p(a["qidx"]),
+            _p(a["qval"]))
+    m, n = lp.m, lp.n
+    out = {k: np.zeros(n) for k in ("c", "l", "u", "C", "Cres")}
+    out.update({k: np.zeros(m) for k in ("lo", "hi", "R", "Rres")})
+    out["a_val"] = np.zeros(lp.A.nnz)
+    scal = np.zeros(7)
+    rc = lib.ora_scale(C.byref(s), int(ruiz_iters), int(pock_chambolle), _p(out["a_val"]), _p(out["c"]),
+                       _p(out["l"]), _p(out["u"]), _p(out["lo"]), _p(out["hi"]), _p(out["R"]), _p(out["C"]),
+                       _p(out["Rres"]), _p(out["Cres"]), _p(scal))
+    if rc != 0:
+        raise RuntimeError("ora_scale failed")
+    for i, k in enumerate(("bscale", "cscale", "norm_a", "norm_q", "bnorm", "cnorm", "obj_const")):
+        out[k] = float(scal[i])
+    return out
+
+
+def plain_iterations(A, AT, c, l, u, lo, hi, tau, sigma, iters, x0, y0):
+    """FP64 PDHG iterations with fixed steps and no restarts (ora_plain_iterations)."""
+    lib = _load(ORACLE_SO)
+    x = np.array(x0, dtype=np.float64, copy=True)
+    y = np.array(y0, dtype=np.float64, copy=True)
+    f = lib.ora_plain_iterations
+    f.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 6 + [C.c_void_p] * 5 + [C.c_double, C.c_double, C.c_long,
+                                                                           C.c_void_p, C.c_void_p]
+    arr = [np.ascontiguousarray(v, dtype=np.float64) for v in (c, l, u, lo, hi)]
+    f(A.rows, A.cols, _p(A.ptr), _p(A.idx), _p(A.val), _p(AT.ptr), _p(AT.idx), _p(AT.val),
+      *[_p(v) for v in arr], float(tau), float(sigma), int(iters), _p(x), _p(y))
+    return x, y
+
+
+# ---------------------------------------------------------------- reference build
+def ref_solve(lp, threads: int | None = None, **opts) -> OracleResult:
+    """Run the UNMODIFIED reference ganit::solve_pdhg_cpu (OpenMP; ``threads``
+    sets omp_set_num_threads through libgomp when given)."""
+    lib = _load(REF_SO)
+    if threads is not None:
+        _set_omp_threads(threads)
+    a = _arrays(lp)
+    o = _options(**opts)
+    r = _RefRes()
+    x = np.zeros(lp.n)
+    y = np.zeros(lp.m)
+    f = lib.ref_solve_pdhg
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 8 + [C.c_double, C.c_int] + [C.c_void_p] * 3 + \
+                 [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    rc = f(lp.m, lp.n, _p(a["ptr"]), _p(a["idx"]), _p(a["val"]), _p(a["c"]), _p(a["l"]), _p(a["u"]), _p(a["lo"]),
+           _p(a["hi"]), float(lp.obj_const), int(lp.maximize), _p(a["qptr"]), _p(a["qidx"]), _p(a["qval"]),
+           C.byref(o), C.byref(r), _p(x), _p(y))
+    if rc != 0:
+        raise RuntimeError("reference solve_pdhg_cpu threw")
+    return OracleResult(STATUS[r.status], r.pobj, r.dobj, r.rel_p, r.rel_d, r.rel_gap, r.iterations,
+                        r.fp32_iterations, r.l2_iterations, r.restarts, r.setup_s, r.solve_s, x, y)
+
+
+def _set_omp_threads(k: int) -> None:
+    gomp = C.CDLL("libgomp.so.1")
+    gomp.omp_set_num_threads(int(k))
+
+
+def ref_read_mps(path: str):
+    """Read an MPS / QPS file with the reference reader (src/mps.cpp:69-272)."""
+    from ganit_v2_b200.lp import LP, Csr
+
+    lib = _load(REF_SO)
+    lib.ref_read_mps.restype = C.c_void_p
+    lib.ref_read_mps.argtypes = [C.c_char_p]
+    h = lib.ref_read_mps(path.encode())
+    if not h:
+        raise RuntimeError(f"reference read_mps failed on {path}")
+    try:
+        dims = np.zeros(5, dtype=np.int64)
+        lib.ref_mps_dims.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ref_mps_dims(h, _p(dims))
+        m, n, nnz, qnnz, maxi = (int(v) for v in dims)
+        ptr = np.zeros(m + 1, np.int32); idx = np.zeros(nnz, np.int32); val = np.zeros(nnz)
+        c = np.zeros(n); l = np.zeros(n); u = np.zeros(n); lo = np.zeros(m); hi = np.zeros(m)
+        oc = np.zeros(1)
+        qptr = np.zeros(n + 1, np.int32) if qnnz else None
+        qidx = np.zeros(qnnz, np.int32) if qnnz else None
+        qval = np.zeros(qnnz) if qnnz else None
+        lib.ref_mps_copy.argtypes = [C.c_void_p] * 13
+        lib.ref_mps_copy(h, _p(ptr), _p(idx), _p(val), _p(c), _p(l), _p(u), _p(lo), _p(hi), _p(oc), _p(qptr),
+                         _p(qidx), _p(qval))
+    finally:
+        lib.ref_mps_free.argtypes = [C.c_void_p]
+        lib.ref_mps_free(h)
+    Q = Csr(n, n, qptr, qidx, qval) if qnnz else None
+    return LP(Csr(m, n, ptr, idx, val), c, l, u, lo, hi, obj_const=float(oc[0]), maximize=bool(maxi), Q=Q,
+              name=os.path.basename(path))
+
+
+def ref_dual_simplex(lp, time_limit: float = 300.0) -> dict:
+    """Exact vertex from the reference DualSimplex: objective, x, row duals y
+    (minimisation sense), basis heads and variable statuses."""
+    lib = _load(REF_SO)
+    a = _arrays(lp)
+    x = np.zeros(lp.n)
+    y = np.zeros(lp.m)
+    head = np.zeros(lp.m, np.int32)
+    status = np.zeros(lp.n + lp.m, np.int8)
+    obj = C.c_double(0)
+    iters = C.c_long(0)
+    f = lib.ref_dual_simplex
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 8 + [C.c_double, C.c_int, C.c_double] + [C.c_void_p] * 6
+    rc = f(lp.m, lp.n, _p(a["ptr"]), _p(a["idx"]), _p(a["val"]), _p(a["c"]), _p(a["l"]), _p(a["u"]), _p(a["lo"]),
+           _p(a["hi"]), float(lp.obj_const), int(lp.maximize), float(time_limit), C.addressof(obj), _p(x), _p(y),
+           _p(head), _p(status), C.addressof(iters))
+    return {"status": int(rc), "objective": obj.value, "x": x, "y": y, "head": head, "var_status": status,
+            "iterations": iters.value}
