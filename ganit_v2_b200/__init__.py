@@ -1,0 +1,14 @@
+"""B200-native restarted-PDHG engine for GANIT's LP / convex-QP path.
+
+Public API (mirrors include/ganit/pdhg.hpp of the reference):
+``Options``, ``Precision``, ``Status``, ``Result``, ``solve_pdhg_gpu`` (alias
+``solve_pdhg_b200``), plus ``Problem`` (resident problem), ``Backend``
+(Backend-concept operations), ``BatchSolver`` and ``DiffBatch``.
+The compute path is libganit_b200.so (sm_100a); there is no CPU fallback.
+"""
+from .lp import LP, Csr
+from .api import (Backend, GanitError, Options, Precision, Problem, Result, Status, load_library, set_device,
+                  solve_pdhg_b200, solve_pdhg_gpu, LIB_PATH)
+
+__all__ = ["LP", "Csr", "Backend", "GanitError", "Options", "Precision", "Problem", "Result", "Status",
+           "load_library", "set_device", "solve_pdhg_b200", "solve_pdhg_gpu", "LIB_PATH"]

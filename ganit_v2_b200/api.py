@@ -1,0 +1,441 @@
+"""Python host API over libganit_b200.so.
+
+Mirrors the reference's public PDHG interface (include/ganit/pdhg.hpp):
+``Precision``, ``Options`` (same fields and defaults), ``Status``, ``Result``
+and ``solve_pdhg_gpu(lp, opt)`` (here backed by the B200 engine; also exported
+as ``solve_pdhg_b200``).  ``Problem`` keeps a scaled problem resident on the
+GPU for repeated solves.  ``Backend`` exposes the Backend-concept operations
+that src/pdhg_impl.hpp drives.
+
+There is no CPU fallback: if the library is missing or no sm_100 GPU is
+visible, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .lp import LP
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libganit_b200.so")
+
+GB_OK = 0
+
+
+class GanitError(RuntimeError):
+    """Error reported by libganit_b200 (status code + message)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libganit_b200 error {code}: {msg}")
+        self.code = code
+
+
+class Precision(enum.IntEnum):  # include/ganit/pdhg.hpp:10
+    Double = 0
+    Mixed = 1
+    Dynamic = 2
+
+
+class Status(enum.IntEnum):  # include/ganit/pdhg.hpp:27
+    Optimal = 0
+    PrimalInfeasible = 1
+    IterationLimit = 2
+    TimeLimit = 3
+    NumericalError = 4
+
+
+STATUS_NAMES = {0: "OPTIMAL", 1: "PRIMAL_INFEASIBLE", 2: "ITERATION_LIMIT", 3: "TIME_LIMIT", 4: "NUMERICAL_ERROR"}
+
+
+@dataclass
+class Options:  # include/ganit/pdhg.hpp:12-25
+    tol: float = 1e-4
+    max_iter: int = 10_000_000
+    time_limit: float = 3600.0
+    check_every: int = 64
+    ruiz_iters: int = 10
+    pock_chambolle: bool = True
+    infeas_tol: float = 1e-8
+    precision: Precision = Precision.Double
+    stall_checks: int = 12
+    stall_checks_l2: int = 24
+    verbose: int = 0
+
+
+@dataclass
+class Result:  # include/ganit/pdhg.hpp:30-42
+    status: Status
+    x: np.ndarray
+    y: np.ndarray
+    pobj: float
+    dobj: float
+    rel_primal: float
+    rel_dual: float
+    rel_gap: float
+    iterations: int
+    fp32_iterations: int
+    l2_iterations: int
+    restarts: int
+    setup_seconds: float
+    solve_seconds: float
+    device: str = "b200"
+    norm_a: float = float("nan")
+    primal_weight: float = float("nan")
+    checks: int = 0
+    phases: int = 0
+
+    @property
+    def status_name(self) -> str:
+        return STATUS_NAMES[int(self.status)]
+
+
+# ---------------------------------------------------------------- ctypes mirror of ganit_b200.h
+class _GbLp(C.Structure):
+    _fields_ = [("m", C.c_int32), ("n", C.c_int32), ("a_ptr", C.c_void_p), ("a_idx", C.c_void_p),
+                ("a_val", C.c_void_p), ("c", C.c_void_p), ("l", C.c_void_p), ("u", C.c_void_p), ("lo", C.c_void_p),
+                ("hi", C.c_void_p), ("obj_const", C.c_double), ("maximize", C.c_int32), ("q_ptr", C.c_void_p),
+                ("q_idx", C.c_void_p), ("q_val", C.c_void_p), ("q_rank", C.c_int32), ("q_F", C.c_void_p),
+                ("q_D", C.c_void_p)]
+
+
+class _GbOptions(C.Structure):
+    _fields_ = [("tol", C.c_double), ("max_iter", C.c_int64), ("time_limit", C.c_double),
+                ("check_every", C.c_int32), ("ruiz_iters", C.c_int32), ("pock_chambolle", C.c_int32),
+                ("infeas_tol", C.c_double), ("precision", C.c_int32), ("stall_checks", C.c_int32),
+                ("stall_checks_l2", C.c_int32), ("verbose", C.c_int32)]
+
+
+class _GbResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("pobj", C.c_double), ("dobj", C.c_double), ("rel_primal", C.c_double),
+                ("rel_dual", C.c_double), ("rel_gap", C.c_double), ("iterations", C.c_int64),
+                ("fp32_iterations", C.c_int64), ("l2_iterations", C.c_int64), ("restarts", C.c_int32),
+                ("setup_seconds", C.c_double), ("solve_seconds", C.c_double), ("norm_a", C.c_double),
+                ("primal_weight", C.c_double), ("checks", C.c_int32), ("phases", C.c_int32)]
+
+
+class _GbScaledLp(C.Structure):
+    _fields_ = [("m", C.c_int32), ("n", C.c_int32)] + [
+        (k, C.c_void_p) for k in ("a_ptr", "a_idx", "a_val", "at_ptr", "at_idx", "at_val", "q_ptr", "q_idx", "q_val",
+                                  "c", "l", "u", "lo", "hi", "rres", "cres")]
+
+
+# Every symbol of include/ganit_b200.h (checked by the tests).
+EXPORTS = [
+    "gb_last_error", "gb_version", "gb_default_options", "gb_set_device", "gb_solve", "gb_problem_create",
+    "gb_problem_solve", "gb_problem_get_solution", "gb_problem_destroy", "gb_problem_stream",
+    "gb_problem_time_kernels", "gb_problem_stats", "gb_backend_create", "gb_backend_destroy", "gb_vec_zeros",
+    "gb_vec_from_host", "gb_vec_to_host", "gb_vec_size", "gb_vec_destroy", "gb_copy", "gb_fill", "gb_spmv_A",
+    "gb_spmv_AT", "gb_spmv_Q", "gb_primal_step", "gb_dual_step", "gb_sub", "gb_scale_into", "gb_primal_res2",
+    "gb_dual_res", "gb_row_dual_obj", "gb_dot", "gb_dot_c", "gb_diff2", "gb_batch_create", "gb_batch_solve",
+    "gb_batch_get_solution", "gb_batch_schedule", "gb_batch_destroy", "gb_diff_create", "gb_diff_forward",
+    "gb_diff_backward", "gb_diff_destroy",
+]
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libganit_b200.so (raises if it is missing -- no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise GanitError(-4, f"{path} is not built; run `python -m ganit_v2_b200.build`")
+    lib = C.CDLL(path)
+    vp, i32, i64, dbl = C.c_void_p, C.c_int, C.c_int64, C.c_double
+    sig = {
+        "gb_last_error": (C.c_char_p, []), "gb_version": (i32, []), "gb_default_options": (None, [vp]),
+        "gb_set_device": (i32, [i32]), "gb_solve": (i32, [vp, vp, vp, vp, vp]),
+        "gb_problem_create": (i32, [vp, vp, vp]), "gb_problem_solve": (i32, [vp, vp, vp]),
+        "gb_problem_get_solution": (i32, [vp, vp, vp]), "gb_problem_destroy": (None, [vp]),
+        "gb_problem_stream": (vp, [vp]), "gb_problem_time_kernels": (i32, [vp, i32, i32, vp, vp, vp]),
+        "gb_problem_stats": (i32, [vp, vp, vp]), "gb_backend_create": (i32, [vp, i32, i32, vp]),
+        "gb_backend_destroy": (None, [vp]), "gb_vec_zeros": (i32, [vp, i32, vp]),
+        "gb_vec_from_host": (i32, [vp, vp, i32, vp]), "gb_vec_to_host": (i32, [vp, vp, vp]),
+        "gb_vec_size": (i32, [vp]), "gb_vec_destroy": (None, [vp]), "gb_copy": (i32, [vp, vp, vp]),
+        "gb_fill": (i32, [vp, vp, dbl]), "gb_spmv_A": (i32, [vp, vp, vp]), "gb_spmv_AT": (i32, [vp, vp, vp]),
+        "gb_spmv_Q": (i32, [vp, vp, vp]), "gb_primal_step": (i32, [vp, vp, vp, vp, dbl, vp, vp, vp]),
+        "gb_dual_step": (i32, [vp, vp, vp, dbl, vp, vp]), "gb_sub": (i32, [vp, vp, vp, vp]),
+        "gb_scale_into": (i32, [vp, vp, dbl, vp]), "gb_primal_res2": (i32, [vp, vp, vp]),
+        "gb_dual_res": (i32, [vp, vp, vp, i32, vp, vp]), "gb_row_dual_obj": (i32, [vp, vp, vp]),
+        "gb_dot": (i32, [vp, vp, vp, vp]), "gb_dot_c": (i32, [vp, vp, vp]), "gb_diff2": (i32, [vp, vp, vp, vp]),
+        "gb_batch_create": (i32, [i32, vp, vp, vp]), "gb_batch_solve": (i32, [vp, vp, vp]),
+        "gb_batch_get_solution": (i32, [vp, i32, vp, vp]), "gb_batch_schedule": (i32, [vp, vp, vp, vp]),
+        "gb_batch_destroy": (None, [vp]), "gb_diff_create": (i32, [i32, vp, vp, i32, i32, vp]),
+        "gb_diff_forward": (i32, [vp, vp, vp, vp, vp]),
+        "gb_diff_backward": (i32, [vp, vp, vp, vp, vp, vp, vp]), "gb_diff_destroy": (None, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(rc: int):
+    if rc != GB_OK:
+        raise GanitError(rc, _lib.gb_last_error().decode(errors="replace"))
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class _LpView:
+    """Keeps the numpy arrays of an LP alive while the C struct points at them."""
+
+    def __init__(self, lp: LP):
+        self.arrays = []
+
+        def keep(a, dt):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=dt)
+            self.arrays.append(a)
+            return a
+
+        ptr = keep(lp.A.ptr, np.int32)
+        idx = keep(lp.A.idx, np.int32)
+        val = keep(lp.A.val, np.float64)
+        vecs = [keep(getattr(lp, k), np.float64) for k in ("c", "l", "u", "lo", "hi")]
+        q = lp.Q if (lp.Q is not None and lp.Q.nnz) else None
+        qp = keep(q.ptr, np.int32) if q else None
+        qi = keep(q.idx, np.int32) if q else None
+        qv = keep(q.val, np.float64) if q else None
+        F = keep(lp.F, np.float64) if lp.F is not None else None
+        D = keep(lp.D, np.float64) if lp.F is not None else None
+        self.s = _GbLp(lp.m, lp.n, _p(ptr), _p(idx), _p(val), *[_p(v) for v in vecs], float(lp.obj_const),
+                       int(lp.maximize), _p(qp), _p(qi), _p(qv), int(F.shape[1]) if F is not None else 0, _p(F),
+                       _p(D))
+
+
+def _opts(opt: Options | None) -> _GbOptions:
+    o = opt or Options()
+    return _GbOptions(o.tol, o.max_iter, o.time_limit, o.check_every, o.ruiz_iters, int(o.pock_chambolle),
+                      o.infeas_tol, int(o.precision), o.stall_checks, o.stall_checks_l2, int(o.verbose))
+
+
+def _result(r: _GbResult, x, y) -> Result:
+    return Result(Status(r.status), x, y, r.pobj, r.dobj, r.rel_primal, r.rel_dual, r.rel_gap, r.iterations,
+                  r.fp32_iterations, r.l2_iterations, r.restarts, r.setup_seconds, r.solve_seconds, "b200",
+                  r.norm_a, r.primal_weight, r.checks, r.phases)
+
+
+def set_device(device: int) -> None:
+    lib = load_library()
+    _check(lib.gb_set_device(int(device)))
+
+
+def solve_pdhg_gpu(lp: LP, opt: Options | None = None) -> Result:
+    """Same contract as ganit::solve_pdhg_gpu (include/ganit/pdhg.hpp:44-47):
+    scale, restarted PDHG with the precision schedule of ``opt``, FP64
+    certification and unscaling -- all on the B200."""
+    lib = load_library()
+    v = _LpView(lp)
+    o = _opts(opt)
+    r = _GbResult()
+    x = np.zeros(lp.n)
+    y = np.zeros(lp.m)
+    _check(lib.gb_solve(C.addressof(v.s), C.addressof(o), C.addressof(r), _p(x), _p(y)))
+    return _result(r, x, y)
+
+
+solve_pdhg_b200 = solve_pdhg_gpu
+
+
+class Problem:
+    """A problem uploaded and scaled once, resident in HBM for repeated solves."""
+
+    def __init__(self, lp: LP, opt: Options | None = None):
+        self._lib = load_library()
+        self.lp = lp
+        self.m, self.n = lp.m, lp.n
+        v = _LpView(lp)
+        o = _opts(opt)
+        h = C.c_void_p()
+        _check(self._lib.gb_problem_create(C.addressof(v.s), C.addressof(o), C.byref(h)))
+        self._h = h
+
+    def solve(self, opt: Options | None = None, fetch: bool = True) -> Result:
+        o = _opts(opt)
+        r = _GbResult()
+        _check(self._lib.gb_problem_solve(self._h, C.addressof(o), C.addressof(r)))
+        x = y = None
+        if fetch:
+            x, y = self.solution()
+        return _result(r, x, y)
+
+    def solution(self):
+        x = np.zeros(self.n)
+        y = np.zeros(self.m)
+        _check(self._lib.gb_problem_get_solution(self._h, _p(x), _p(y)))
+        return x, y
+
+    def time_kernels(self, level: int, iters: int = 50):
+        mp, md = C.c_double(), C.c_double()
+        nl = C.c_int64()
+        _check(self._lib.gb_problem_time_kernels(self._h, int(level), int(iters), C.byref(mp), C.byref(md),
+                                                 C.byref(nl)))
+        return mp.value, md.value, nl.value
+
+    def stats(self):
+        nl = C.c_int64()
+        bpi = np.zeros(3)
+        _check(self._lib.gb_problem_stats(self._h, C.byref(nl), _p(bpi)))
+        return nl.value, bpi
+
+    @property
+    def stream(self) -> int:
+        return self._lib.gb_problem_stream(self._h) or 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.gb_problem_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+# ---------------------------------------------------------------- Backend concept
+class Vec:
+    def __init__(self, be: "Backend", h):
+        self.be = be
+        self._h = h
+
+    @property
+    def size(self) -> int:
+        return self.be._lib.gb_vec_size(self._h)
+
+    def to_host(self) -> np.ndarray:
+        out = np.zeros(self.size)
+        _check(self.be._lib.gb_vec_to_host(self.be._h, self._h, _p(out)))
+        return out
+
+    def __del__(self):
+        try:
+            if self._h:
+                self.be._lib.gb_vec_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+class Backend:
+    """The Backend concept of src/pdhg_impl.hpp on B200 kernels.
+
+    ``scaled`` is a dict with the ScaledLP arrays (src/scaling.hpp:8-23):
+    A, AT (Csr), optional Q (Csr), c, l, u, lo, hi, Rres, Cres.  ``mat`` and
+    ``vec`` are "f32" / "f64" (L1 = f32/f32, L2 = f32/f64, L3 = f64/f64)."""
+
+    def __init__(self, scaled: dict, mat: str = "f64", vec: str = "f64"):
+        self._lib = load_library()
+        self._keep = []
+
+        def k(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            self._keep.append(a)
+            return _p(a)
+
+        A, AT, Q = scaled["A"], scaled["AT"], scaled.get("Q")
+        self.m, self.n = A.rows, A.cols
+        s = _GbScaledLp(A.rows, A.cols, k(A.ptr, np.int32), k(A.idx, np.int32), k(A.val, np.float64),
+                        k(AT.ptr, np.int32), k(AT.idx, np.int32), k(AT.val, np.float64),
+                        k(Q.ptr, np.int32) if Q is not None else None, k(Q.idx, np.int32) if Q is not None else None,
+                        k(Q.val, np.float64) if Q is not None else None,
+                        *[k(scaled[n], np.float64) for n in ("c", "l", "u", "lo", "hi", "Rres", "Cres")])
+        h = C.c_void_p()
+        _check(self._lib.gb_backend_create(C.addressof(s), 0 if mat == "f32" else 1, 0 if vec == "f32" else 1,
+                                           C.byref(h)))
+        self._h = h
+
+    def zeros(self, k: int) -> Vec:
+        h = C.c_void_p()
+        _check(self._lib.gb_vec_zeros(self._h, int(k), C.byref(h)))
+        return Vec(self, h)
+
+    def from_host(self, a) -> Vec:
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        h = C.c_void_p()
+        _check(self._lib.gb_vec_from_host(self._h, _p(a), int(a.shape[0]), C.byref(h)))
+        return Vec(self, h)
+
+    def to_host(self, v: Vec) -> np.ndarray:
+        return v.to_host()
+
+    def copy(self, src: Vec, dst: Vec):
+        _check(self._lib.gb_copy(self._h, src._h, dst._h))
+
+    def fill(self, v: Vec, a: float):
+        _check(self._lib.gb_fill(self._h, v._h, float(a)))
+
+    def spmv_A(self, x, ax):
+        _check(self._lib.gb_spmv_A(self._h, x._h, ax._h))
+
+    def spmv_AT(self, y, aty):
+        _check(self._lib.gb_spmv_AT(self._h, y._h, aty._h))
+
+    def spmv_Q(self, x, qx):
+        _check(self._lib.gb_spmv_Q(self._h, x._h, qx._h))
+
+    def primal_step(self, x, aty, qx, tau, xn, xbar, sumx):
+        _check(self._lib.gb_primal_step(self._h, x._h, aty._h, qx._h if qx is not None else None, float(tau),
+                                        xn._h, xbar._h, sumx._h))
+
+    def dual_step(self, y, axbar, sigma, yn, sumy):
+        _check(self._lib.gb_dual_step(self._h, y._h, axbar._h, float(sigma), yn._h, sumy._h))
+
+    def sub(self, a, b, d):
+        _check(self._lib.gb_sub(self._h, a._h, b._h, d._h))
+
+    def scale_into(self, src, a, dst):
+        _check(self._lib.gb_scale_into(self._h, src._h, float(a), dst._h))
+
+    def _r1(self, fn, *args):
+        out = C.c_double()
+        _check(fn(self._h, *args, C.byref(out)))
+        return out.value
+
+    def primal_res2(self, ax):
+        return self._r1(self._lib.gb_primal_res2, ax._h)
+
+    def dual_res(self, aty, qx=None, with_c=True):
+        a, b = C.c_double(), C.c_double()
+        _check(self._lib.gb_dual_res(self._h, aty._h, qx._h if qx is not None else None, int(with_c), C.byref(a),
+                                     C.byref(b)))
+        return a.value, b.value
+
+    def row_dual_obj(self, y):
+        return self._r1(self._lib.gb_row_dual_obj, y._h)
+
+    def dot(self, a, b):
+        return self._r1(self._lib.gb_dot, a._h, b._h)
+
+    def dot_c(self, x):
+        return self._r1(self._lib.gb_dot_c, x._h)
+
+    def diff2(self, a, b):
+        return self._r1(self._lib.gb_diff2, a._h, b._h)
+
+    def __del__(self):
+        try:
+            if self._h:
+                self._lib.gb_backend_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass

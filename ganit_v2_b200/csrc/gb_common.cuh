@@ -1,0 +1,126 @@
+// Common pieces of the B200 PDHG engine: error plumbing, device buffers,
+// deterministic block reductions.  Built with -fmad=false so that every
+// vector update rounds exactly like the reference's scalar C++ code
+// (src/backend_cpu.cpp), i.e. no silent FMA contraction.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace gb {
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define GB_CUDA(call)                                                                                   \
+    do {                                                                                                \
+        cudaError_t e__ = (call);                                                                       \
+        if (e__ != cudaSuccess)                                                                         \
+            throw ::gb::Error(e__ == cudaErrorMemoryAllocation ? -3 : -2,                               \
+                              std::string("CUDA error ") + cudaGetErrorString(e__) + " at " __FILE__ ":" + \
+                                  std::to_string(__LINE__));                                            \
+    } while (0)
+
+#define GB_REQUIRE(cond, msg)                                        \
+    do {                                                             \
+        if (!(cond)) throw ::gb::Error(-1, std::string(msg));        \
+    } while (0)
+
+// Owning device buffer (move-only).
+template <class T>
+class DevBuf {
+   public:
+    DevBuf() = default;
+    explicit DevBuf(size_t n) { reset(n); }
+    ~DevBuf() { release(); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; o.n_ = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        std::swap(p_, o.p_);
+        std::swap(n_, o.n_);
+        return *this;
+    }
+    void reset(size_t n) {
+        release();
+        n_ = n;
+        if (n_) GB_CUDA(cudaMalloc(&p_, n_ * sizeof(T)));
+    }
+    void release() {
+        if (p_) cudaFree(p_);
+        p_ = nullptr;
+        n_ = 0;
+    }
+    T* get() const { return p_; }
+    size_t size() const { return n_; }
+    void upload(const T* h, size_t n, cudaStream_t s) {
+        if (n) GB_CUDA(cudaMemcpyAsync(p_, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void download(T* h, size_t n, cudaStream_t s) const {
+        if (n) GB_CUDA(cudaMemcpyAsync(h, p_, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+    }
+
+   private:
+    T* p_ = nullptr;
+    size_t n_ = 0;
+};
+
+constexpr int kThreads = 256;  // CTA size of every streaming kernel
+constexpr int kWarps = kThreads / 32;
+
+inline int div_up(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
+__host__ __device__ __forceinline__ int div_up_dev(int a, int b) { return (a + b - 1) / b; }
+
+// grid for an elementwise kernel: at most 8 CTAs per SM worth of work per
+// launch, grid-stride beyond that (148 SMs on B200).
+inline int elem_grid(long long n, int sms) {
+    long long g = (n + kThreads - 1) / kThreads;
+    long long cap = static_cast<long long>(sms) * 8;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return static_cast<int>(g);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Deterministic block sum of K doubles held by every thread.  Result valid in
+// thread 0.  `sh` must hold kWarps*K doubles.  Order: shuffle tree inside each
+// warp, then warps 0..7 sequentially.
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double* sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double t = warp_sum(v[k]);
+        if (lane == 0) sh[wid * K + k] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double t = 0.0;
+            for (int w = 0; w < kWarps; ++w) t += sh[w * K + k];
+            v[k] = t;
+        }
+    }
+    __syncthreads();
+}
+
+}  // namespace gb

@@ -1,0 +1,523 @@
+// Fused restarted-PDHG kernels for one problem instance.
+//
+// Per iteration (src/pdhg_impl.hpp:133-139) two launches:
+//   k_primal : rows j of the stored transpose: aty_j = (A^T y)_j, then the
+//              primal step of src/backend_cpu.cpp:67-80 in the epilogue
+//              (x+ = clamp(x - tau (c - aty + qx)), xbar = 2x+ - x, sumx += x+)
+//   k_dual   : rows i of A: ax_i = (A xbar)_i, then the dual step of
+//              src/backend_cpu.cpp:81-92 (y+ = q + clamp(-q, sigma lo, sigma hi))
+// Every check_every iterations (pdhg_impl.hpp:142-190) one k_eval launch
+// computes, for the current iterate, the running average and the ray y - y_r,
+// all KKT pieces of pdhg_impl.hpp:92-118 in FP64 (one pass over A and one
+// over A^T, several right-hand sides per pass), and its last CTA reduces the
+// per-CTA partials in a fixed order and runs the whole scalar decision of
+// pdhg_impl.hpp:144-189 (convergence, limits, infeasibility certificate,
+// stall exit, adaptive restart, primal-weight update).  k_restart applies a
+// restart.  No host round trip happens inside a precision phase.
+#pragma once
+#include "gb_spmv.cuh"
+
+namespace gb {
+
+struct Kkt {
+    double pobj, dobj, rel_p, rel_d, rel_gap, err;
+};
+
+// Phase exits (pdhg_impl.hpp:65)
+enum PhaseExit : int { kConverged = 0, kStalled = 1, kIterLimit = 2, kTimeLimit = 3, kInfeasible = 4, kNumerical = 5 };
+enum EvalMode : int { kEvalInit = 0, kEvalCheck = 1, kEvalCertify = 2 };
+
+// Device-resident solver state (PdhgShared + PdhgState + loop locals of
+// pdhg_impl.hpp:44-63, 120-128).  Scalars are FP64.
+struct alignas(16) SolveState {
+    // problem constants
+    double eta, normA, normQ, obj_scale, obj_const, bnorm, cnorm;
+    double phase_tol, infeas_tol, time_limit_s;
+    long long max_iter;
+    int check_every, stall_checks, stall_exit, has_q;
+    unsigned long long t0_ns;
+    // carried across phases (PdhgState)
+    double w;
+    long long it;
+    int restarts;
+    int checks;
+    double carry_restart_err;  // st.restart_err (-1 = none)
+    // phase loop locals
+    double tau, sigma;
+    long long it_since;
+    double restart_err, prev_cand, best_err;
+    int cwp;                   // checks without progress
+    // decision of the last check
+    int restart_now, avg_better, done, exit_reason, best_is_avg;
+    double inv_avg;
+    Kkt best, kcert, kc, ka;
+    unsigned arrive;           // CTA arrival counter of k_eval (re-armed by the last CTA)
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// ---------------------------------------------------------------- iteration kernels
+template <class M, class V>
+struct PrimalArgs {
+    CsrView<M> AT;
+    const V* __restrict__ y;     // gathered by column index of A^T (row of A)
+    const V* __restrict__ x;
+    const V* __restrict__ c;
+    const V* __restrict__ l;
+    const V* __restrict__ u;
+    const V* __restrict__ qx;    // Q x or nullptr
+    V* __restrict__ xn;
+    V* __restrict__ xbar;
+    V* __restrict__ sumx;
+    const SolveState* st;
+};
+
+template <class M, class V>
+struct PrimalEpi {
+    const PrimalArgs<M, V>& a;
+    V tau;
+    __device__ __forceinline__ void operator()(int j, const V (&s)[1]) {
+        const V xj = a.x[j];
+        const V g = a.c[j] - s[0] + (a.qx ? a.qx[j] : V(0));
+        V v = xj - tau * g;
+        const V lj = a.l[j], uj = a.u[j];
+        v = (v < lj) ? lj : v;
+        v = (uj < v) ? uj : v;
+        a.xn[j] = v;
+        a.xbar[j] = V(2) * v - xj;
+        a.sumx[j] += v;
+    }
+};
+
+template <class M, class V>
+__global__ void __launch_bounds__(kThreads) k_primal(const PrimalArgs<M, V> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const RowBlock b = a.AT.blocks[blockIdx.x];
+    PrimalEpi<M, V> epi{a, static_cast<V>(a.st->tau)};
+    spmv_block<1, M, V>(a.AT, b, GatherOne<V>{a.y}, epi, smem);
+}
+
+template <class M, class V>
+struct DualArgs {
+    CsrView<M> A;
+    const V* __restrict__ xbar;
+    const V* __restrict__ y;
+    const V* __restrict__ lo;
+    const V* __restrict__ hi;
+    V* __restrict__ yn;
+    V* __restrict__ sumy;
+    const SolveState* st;
+};
+
+template <class M, class V>
+struct DualEpi {
+    const DualArgs<M, V>& a;
+    V sigma;
+    __device__ __forceinline__ void operator()(int i, const V (&s)[1]) {
+        const V q = a.y[i] - sigma * s[0];
+        const V lo = sigma * a.lo[i], hi = sigma * a.hi[i];
+        V t = -q;
+        t = (t < lo) ? lo : t;
+        t = (hi < t) ? hi : t;
+        const V v = q + t;
+        a.yn[i] = v;
+        a.sumy[i] += v;
+    }
+};
+
+template <class M, class V>
+__global__ void __launch_bounds__(kThreads) k_dual(const DualArgs<M, V> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const RowBlock b = a.A.blocks[blockIdx.x];
+    DualEpi<M, V> epi{a, static_cast<V>(a.st->sigma)};
+    spmv_block<1, M, V>(a.A, b, GatherOne<V>{a.xbar}, epi, smem);
+}
+
+// ---------------------------------------------------------------- KKT evaluation
+// FP64 partial sums written by every CTA of k_eval.
+enum Term : int {
+    T_RP2_C = 0, T_RP2_A, T_ROBJ_C, T_ROBJ_A, T_ROBJ_R, T_DY2_C, T_DY2_A,
+    T_RD2_C, T_VOBJ_C, T_RD2_A, T_VOBJ_A, T_RD2_R, T_VOBJ_R, T_CX_C, T_CX_A, T_XQX_C, T_XQX_A, T_DX2_C, T_DX2_A,
+    kTerms
+};
+
+template <class M, class V>
+struct EvalArgs {
+    CsrView<M> A, AT;
+    const V* __restrict__ x;
+    const V* __restrict__ y;
+    const V* __restrict__ sumx;
+    const V* __restrict__ sumy;
+    const V* __restrict__ xr;
+    const V* __restrict__ yr;
+    const V* __restrict__ c;
+    const V* __restrict__ l;
+    const V* __restrict__ u;
+    const V* __restrict__ lo;
+    const V* __restrict__ hi;
+    const V* __restrict__ rres;
+    const V* __restrict__ cres;
+    const V* __restrict__ qx;    // Q x   (QP) or nullptr
+    const V* __restrict__ qxa;   // Q xa  (QP, check mode) or nullptr
+    int mode;
+    SolveState* st;
+    double* partials;            // [gridDim.x][kTerms]
+    unsigned long long cond;     // cudaGraphConditionalHandle of the phase loop
+    int use_cond;                // 1 inside the loop body: the decision drives the loop
+};
+
+template <class V>
+__device__ __forceinline__ V avg_of(const V* s, int k, double inv) {
+    return static_cast<V>(inv * static_cast<double>(s[k]));  // scale_into, backend_cpu.cpp:97-100
+}
+
+template <class V, int NV>
+struct GatherXAvg {  // A side: x and (check) the running average xa
+    const V* __restrict__ x;
+    const V* __restrict__ sumx;
+    double inv;
+    __device__ __forceinline__ void operator()(int j, V (&o)[NV]) const {
+        o[0] = __ldg(x + j);
+        if (NV > 1) o[NV > 1 ? 1 : 0] = avg_of(sumx, j, inv);
+    }
+};
+
+template <class V, int NV>
+struct GatherYAvgRay {  // A^T side: y, ya and the ray y - yr
+    const V* __restrict__ y;
+    const V* __restrict__ sumy;
+    const V* __restrict__ yr;
+    double inv;
+    __device__ __forceinline__ void operator()(int i, V (&o)[NV]) const {
+        const V yi = __ldg(y + i);
+        o[0] = yi;
+        if (NV > 1) {
+            o[NV > 1 ? 1 : 0] = avg_of(sumy, i, inv);
+            o[NV > 2 ? 2 : 0] = yi - __ldg(yr + i);
+        }
+    }
+};
+
+// Per-row terms (backend_cpu.cpp:101-112, 132-142) and restart distances.
+template <class M, class V, int NV>
+struct EvalRowEpi {
+    const EvalArgs<M, V>& a;
+    double inv;
+    double t[kTerms];
+    __device__ __forceinline__ static double pres2(double ax, double lo, double hi, double r) {
+        double p = (ax < lo) ? lo : ax;
+        p = (hi < p) ? hi : p;
+        const double d = (ax - p) / r;
+        return d * d;
+    }
+    __device__ __forceinline__ static double robj(double yi, double lo, double hi) {
+        if (yi > 0 && isfinite(lo)) return yi * lo;
+        if (yi < 0 && isfinite(hi)) return yi * hi;
+        return 0.0;
+    }
+    __device__ __forceinline__ void operator()(int i, const V (&s)[NV]) {
+        const double lo = double(a.lo[i]), hi = double(a.hi[i]), r = double(a.rres[i]);
+        const V yi = a.y[i];
+        t[T_RP2_C] += pres2(double(s[0]), lo, hi, r);
+        t[T_ROBJ_C] += robj(double(yi), lo, hi);
+        if (NV > 1) {
+            const V ya = avg_of(a.sumy, i, inv);
+            const V yri = a.yr[i];
+            const V ray = yi - yri;
+            t[T_RP2_A] += pres2(double(s[NV > 1 ? 1 : 0]), lo, hi, r);
+            t[T_ROBJ_A] += robj(double(ya), lo, hi);
+            t[T_ROBJ_R] += robj(double(ray), lo, hi);
+            const double d0 = double(yi) - double(yri), d1 = double(ya) - double(yri);
+            t[T_DY2_C] += d0 * d0;
+            t[T_DY2_A] += d1 * d1;
+        }
+    }
+};
+
+// Per-column terms (backend_cpu.cpp:113-131, 143-149).
+template <class M, class V, int NV>
+struct EvalColEpi {
+    const EvalArgs<M, V>& a;
+    double inv;
+    double t[kTerms];
+    __device__ __forceinline__ static void dres(double z, double lj, double uj, double cres, double& rd2,
+                                                double& ob) {
+        double r = 0.0;
+        if (z > 0) { if (isfinite(lj)) ob += z * lj; else r = z; }
+        else if (z < 0) { if (isfinite(uj)) ob += z * uj; else r = z; }
+        r /= cres;
+        rd2 += r * r;
+    }
+    __device__ __forceinline__ void operator()(int j, const V (&s)[NV]) {
+        const double cj = double(a.c[j]), lj = double(a.l[j]), uj = double(a.u[j]), cr = double(a.cres[j]);
+        const V xj = a.x[j];
+        const double qc = a.qx ? double(a.qx[j]) : 0.0;
+        dres(1.0 * cj - double(s[0]) + qc, lj, uj, cr, t[T_RD2_C], t[T_VOBJ_C]);
+        t[T_CX_C] += cj * double(xj);
+        if (a.qx) t[T_XQX_C] += double(xj) * qc;
+        if (NV > 1) {
+            const V xa = avg_of(a.sumx, j, inv);
+            const V xrj = a.xr[j];
+            const double qa = a.qxa ? double(a.qxa[j]) : 0.0;
+            dres(1.0 * cj - double(s[NV > 1 ? 1 : 0]) + qa, lj, uj, cr, t[T_RD2_A], t[T_VOBJ_A]);
+            dres(0.0 * cj - double(s[NV > 2 ? 2 : 0]) + 0.0, lj, uj, cr, t[T_RD2_R], t[T_VOBJ_R]);
+            t[T_CX_A] += cj * double(xa);
+            if (a.qxa) t[T_XQX_A] += double(xa) * qa;
+            const double d0 = double(xj) - double(xrj), d1 = double(xa) - double(xrj);
+            t[T_DX2_C] += d0 * d0;
+            t[T_DX2_A] += d1 * d1;
+        }
+    }
+};
+
+// KKT from reduced terms (eval lambda, pdhg_impl.hpp:102-107)
+__device__ __forceinline__ Kkt make_kkt(const SolveState& s, double cx, double xqx, double robj, double vobj,
+                                        double rp2, double rd2) {
+    Kkt k;
+    k.pobj = (cx + 0.5 * xqx) * s.obj_scale + s.obj_const;
+    k.dobj = (robj + vobj - 0.5 * xqx) * s.obj_scale + s.obj_const;
+    k.rel_p = sqrt(rp2) / (1.0 + s.bnorm);
+    k.rel_d = sqrt(rd2) / (1.0 + s.cnorm);
+    k.rel_gap = fabs(k.pobj - k.dobj) / (1.0 + fabs(k.pobj) + fabs(k.dobj));
+    k.err = sqrt(k.rel_p * k.rel_p + k.rel_d * k.rel_d + k.rel_gap * k.rel_gap);
+    return k;
+}
+__device__ __forceinline__ bool kkt_finite(const Kkt& k) {
+    return isfinite(k.pobj) && isfinite(k.dobj) && isfinite(k.rel_p) && isfinite(k.rel_d);
+}
+__device__ __forceinline__ bool kkt_conv(const Kkt& k, double tol) {
+    return k.rel_p <= tol && k.rel_d <= tol && k.rel_gap <= tol;
+}
+
+__device__ __forceinline__ void step_sizes(SolveState& s) {  // pdhg_impl.hpp:87-91
+    s.sigma = s.eta * s.w;
+    s.tau = s.eta / s.w;
+    if (s.has_q) {
+        const double tq = 0.998 / (0.5 * s.normQ + s.sigma * s.normA * s.normA);
+        s.tau = (tq < s.tau) ? tq : s.tau;
+    }
+}
+
+// Scalar decision logic, run by one thread after all partials are reduced.
+static __device__ void decide(SolveState& s, const double (&T)[kTerms], int mode) {
+    const Kkt kc = make_kkt(s, T[T_CX_C], T[T_XQX_C], T[T_ROBJ_C], T[T_VOBJ_C], T[T_RP2_C], T[T_RD2_C]);
+    if (mode == kEvalCertify) { s.kcert = kc; return; }
+    if (mode == kEvalInit) {  // pdhg_impl.hpp:120-128
+        double e = kc.err;
+        if (s.carry_restart_err > 0) e = (e < s.carry_restart_err) ? s.carry_restart_err : e;
+        s.restart_err = e;
+        s.prev_cand = INFINITY;
+        s.it_since = 0;
+        s.best_err = e;
+        s.cwp = 0;
+        s.done = 0;
+        s.exit_reason = kIterLimit;
+        s.best_is_avg = 0;
+        s.restart_now = 0;
+        s.avg_better = 0;
+        s.kc = kc;
+        step_sizes(s);
+        if (s.t0_ns == 0) s.t0_ns = global_ns();
+        return;
+    }
+    // check (pdhg_impl.hpp:144-189)
+    const long long it = s.it + s.check_every;
+    const long long it_since = s.it_since + s.check_every;
+    s.it = it;
+    s.checks += 1;
+    s.inv_avg = 1.0 / static_cast<double>(it_since);
+    const Kkt ka = make_kkt(s, T[T_CX_A], T[T_XQX_A], T[T_ROBJ_A], T[T_VOBJ_A], T[T_RP2_A], T[T_RD2_A]);
+    s.kc = kc;
+    s.ka = ka;
+    s.restart_now = 0;
+    const double t = (global_ns() - s.t0_ns) * 1e-9;
+    int done = 1;
+    const bool avg_better = kkt_finite(ka) && (!kkt_finite(kc) || ka.err < kc.err);
+    const Kkt kcand = avg_better ? ka : kc;
+    if (!kkt_finite(kc) && !kkt_finite(ka)) { s.exit_reason = kNumerical; s.best = kc; s.best_is_avg = 0; }
+    else if (kkt_conv(kc, s.phase_tol)) { s.exit_reason = kConverged; s.best = kc; s.best_is_avg = 0; }
+    else if (kkt_conv(ka, s.phase_tol)) { s.exit_reason = kConverged; s.best = ka; s.best_is_avg = 1; }
+    else if (it >= s.max_iter) { s.exit_reason = kIterLimit; s.best = kcand; s.best_is_avg = avg_better; }
+    else if (t >= s.time_limit_s) { s.exit_reason = kTimeLimit; s.best = kcand; s.best_is_avg = avg_better; }
+    else {
+        bool infeasible = false;
+        if (it_since >= 4LL * s.check_every) {  // primal_infeasible (pdhg_impl.hpp:110-118)
+            const double dray = (T[T_ROBJ_R] + T[T_VOBJ_R]) * s.obj_scale;
+            infeasible = (dray > 0) && sqrt(T[T_RD2_R]) * (1.0 + s.bnorm) / dray <= s.infeas_tol;
+        }
+        if (infeasible) { s.exit_reason = kInfeasible; s.best = kcand; s.best_is_avg = avg_better; }
+        else {
+            done = 0;
+            if (kcand.err < 0.8 * s.best_err) { s.best_err = kcand.err; s.cwp = 0; }
+            else if (++s.cwp >= s.stall_checks && s.stall_exit) {
+                done = 1;
+                s.exit_reason = kStalled; s.best = kcand; s.best_is_avg = avg_better;
+            }
+        }
+    }
+    s.done = done;
+    s.avg_better = avg_better;
+    s.it_since = it_since;
+    if (!done) {  // adaptive restart (pdhg_impl.hpp:172-189)
+        const bool sufficient = kcand.err <= 0.2 * s.restart_err;
+        const bool necessary = kcand.err <= 0.8 * s.restart_err && kcand.err > s.prev_cand;
+        const bool artificial = static_cast<double>(it_since) >= 0.36 * static_cast<double>(it);
+        s.prev_cand = kcand.err;
+        if (sufficient || necessary || artificial) {
+            const double dx = sqrt(avg_better ? T[T_DX2_A] : T[T_DX2_C]);
+            const double dy = sqrt(avg_better ? T[T_DY2_A] : T[T_DY2_C]);
+            if (dx > 1e-10 && dy > 1e-10) s.w = exp(0.5 * log(dy / dx) + 0.5 * log(s.w));
+            s.restart_now = 1;
+            s.it_since = 0;
+            s.restart_err = kcand.err;
+            s.prev_cand = INFINITY;
+            s.restarts += 1;
+        }
+        step_sizes(s);
+    }
+}
+
+template <class M, class V, int NVA, int NVT>
+__global__ void __launch_bounds__(kThreads) k_eval(const EvalArgs<M, V> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double red[kWarps * kTerms];
+    __shared__ bool am_last;
+    const int nbA = a.A.nb;
+    const double inv = (a.mode == kEvalCheck)
+                           ? 1.0 / static_cast<double>(a.st->it_since + a.st->check_every)
+                           : 0.0;
+    double t[kTerms];
+    if (static_cast<int>(blockIdx.x) < nbA) {
+        const RowBlock b = a.A.blocks[blockIdx.x];
+        EvalRowEpi<M, V, NVA> epi{a, inv, {}};
+#pragma unroll
+        for (int k = 0; k < kTerms; ++k) epi.t[k] = 0.0;
+        spmv_block<NVA, M, V>(a.A, b, GatherXAvg<V, NVA>{a.x, a.sumx, inv}, epi, smem);
+#pragma unroll
+        for (int k = 0; k < kTerms; ++k) t[k] = epi.t[k];
+    } else {
+        const RowBlock b = a.AT.blocks[blockIdx.x - nbA];
+        EvalColEpi<M, V, NVT> epi{a, inv, {}};
+#pragma unroll
+        for (int k = 0; k < kTerms; ++k) epi.t[k] = 0.0;
+        spmv_block<NVT, M, V>(a.AT, b, GatherYAvgRay<V, NVT>{a.y, a.sumy, a.yr, inv}, epi, smem);
+#pragma unroll
+        for (int k = 0; k < kTerms; ++k) t[k] = epi.t[k];
+    }
+    block_sum<kTerms>(t, red);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < kTerms; ++k) a.partials[static_cast<size_t>(blockIdx.x) * kTerms + k] = t[k];
+        __threadfence();
+        const unsigned prev = atomicAdd(&a.st->arrive, 1u);
+        am_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!am_last) return;
+    // last CTA: fixed-order reduction of all partials, then the decision
+    __threadfence();
+    double T[kTerms];
+#pragma unroll
+    for (int k = 0; k < kTerms; ++k) T[k] = 0.0;
+    for (int blk = threadIdx.x; blk < static_cast<int>(gridDim.x); blk += kThreads) {
+#pragma unroll
+        for (int k = 0; k < kTerms; ++k) T[k] += __ldcg(a.partials + static_cast<size_t>(blk) * kTerms + k);
+    }
+    block_sum<kTerms>(T, red);
+    if (threadIdx.x == 0) {
+        SolveState& s = *a.st;
+        s.arrive = 0u;
+        decide(s, T, a.mode);
+        if (a.use_cond) {
+            cudaGraphSetConditional(static_cast<cudaGraphConditionalHandle>(a.cond),
+                                    (a.mode == kEvalCheck && s.done) ? 0u : 1u);
+        }
+    }
+}
+
+// Restart / buffer bookkeeping after a check (pdhg_impl.hpp:178-185).
+// `xc`/`yc` hold the current iterate (buffer 1 when check_every is odd);
+// the result always lands in buffer 0 (x0, y0).
+template <class V>
+struct RestartArgs {
+    const V* xc; const V* yc;
+    V* x0; V* y0; V* xr; V* yr; V* sumx; V* sumy;
+    int n, m;
+    const SolveState* st;
+};
+
+template <class V>
+__global__ void k_restart(const RestartArgs<V> a) {
+    const SolveState& s = *a.st;
+    const bool restart = s.restart_now != 0;
+    const bool copy = a.xc != a.x0;
+    if (!restart && !copy) return;
+    const bool avg = s.avg_better != 0;
+    const double inv = s.inv_avg;
+    const int stride = gridDim.x * blockDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < a.n; j += stride) {
+        V v = a.xc[j];
+        if (restart) {
+            if (avg) v = avg_of(a.sumx, j, inv);
+            a.xr[j] = v;
+            a.sumx[j] = V(0);
+        }
+        a.x0[j] = v;
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.m; i += stride) {
+        V v = a.yc[i];
+        if (restart) {
+            if (avg) v = avg_of(a.sumy, i, inv);
+            a.yr[i] = v;
+            a.sumy[i] = V(0);
+        }
+        a.y0[i] = v;
+    }
+}
+
+// Phase start: iterate, restart point and zero sums in precision V from the
+// FP64 carried state (pdhg_impl.hpp:78-84).
+template <class V>
+__global__ void k_phase_in(int n, int m, const double* x64, const double* y64, const double* xr64,
+                           const double* yr64, V* x, V* y, V* xr, V* yr, V* sumx, V* sumy) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        x[j] = static_cast<V>(x64[j]);
+        xr[j] = static_cast<V>(xr64[j]);
+        sumx[j] = V(0);
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        y[i] = static_cast<V>(y64[i]);
+        yr[i] = static_cast<V>(yr64[i]);
+        sumy[i] = V(0);
+    }
+}
+
+// Phase end: best point (current or average) and restart point to FP64
+// (pdhg_impl.hpp:191-194).
+template <class V>
+__global__ void k_phase_out(int n, int m, const V* x, const V* y, const V* sumx, const V* sumy, const V* xr,
+                            const V* yr, const SolveState* st, double* x64, double* y64, double* xr64,
+                            double* yr64) {
+    const bool avg = st->best_is_avg != 0;
+    const double inv = st->inv_avg;
+    const int stride = gridDim.x * blockDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        x64[j] = static_cast<double>(avg ? avg_of(sumx, j, inv) : x[j]);
+        xr64[j] = static_cast<double>(xr[j]);
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        y64[i] = static_cast<double>(avg ? avg_of(sumy, i, inv) : y[i]);
+        yr64[i] = static_cast<double>(yr[i]);
+    }
+}
+
+static __global__ void k_mark_start(SolveState* st) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) st->t0_ns = global_ns();
+}
+
+}  // namespace gb

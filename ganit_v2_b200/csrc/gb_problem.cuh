@@ -1,0 +1,110 @@
+// Host-side engine for one resident problem: upload, device setup, precision
+// phases driven by per-level CUDA graphs whose body (check_every iterations +
+// KKT check + restart) repeats inside a device-side while loop.
+#pragma once
+#include <chrono>
+#include <memory>
+
+#include "../../include/ganit_b200.h"
+#include "gb_pdhg.cuh"
+#include "gb_setup.cuh"
+
+namespace gb {
+
+struct DevMat {
+    int rows = 0, cols = 0;
+    long long nnz = 0;
+    DevBuf<int> ptr, idx;
+    DevBuf<double> val64;
+    DevBuf<float> val32;
+    DevSchedule sched;
+    std::vector<int> host_ptr;
+    template <class M>
+    CsrView<M> view() const {
+        CsrView<M> v;
+        v.ptr = ptr.get();
+        v.idx = idx.get();
+        v.val = val<M>();
+        v.blocks = sched.blocks.get();
+        v.slots = sched.slots.get();
+        v.counters = sched.counters.get();
+        v.rows = rows;
+        v.nb = sched.nb;
+        return v;
+    }
+    template <class M>
+    const M* val() const;
+};
+template <>
+inline const double* DevMat::val<double>() const { return val64.get(); }
+template <>
+inline const float* DevMat::val<float>() const { return val32.get(); }
+
+// Problem data and iterate buffers in vector precision V.
+template <class V>
+struct VecSet {
+    DevBuf<V> c, l, u, lo, hi, rres, cres;
+    DevBuf<V> x0, x1, xbar, y0, y1, sumx, sumy, xr, yr, qx, qxa;
+    DevBuf<V> F, D;  // DPLR factor (n x k) and diagonal in precision V
+    DevBuf<V> ftx;   // F^T x partials / results (QP)
+    void alloc(int n, int m, int qk, bool has_q) {
+        for (DevBuf<V>* b : {&c, &l, &u, &cres, &x0, &x1, &xbar, &sumx, &xr}) b->reset(n ? n : 1);
+        for (DevBuf<V>* b : {&lo, &hi, &rres, &y0, &y1, &sumy, &yr}) b->reset(m ? m : 1);
+        if (has_q) {
+            qx.reset(n ? n : 1);
+            qxa.reset(n ? n : 1);
+        }
+        if (qk > 0) {
+            F.reset(static_cast<size_t>(n) * qk);
+            D.reset(n);
+            ftx.reset(static_cast<size_t>(2) * qk);
+        }
+    }
+};
+
+struct LevelGraph {
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    int check_every = 0;
+    long long launches_per_body = 0;
+    ~LevelGraph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+struct Problem {
+    int device = 0, sms = 148;
+    cudaStream_t stream = nullptr;
+    int m = 0, n = 0;
+    bool maximize = false;
+    double obj_const = 0.0;
+    DevMat A, AT, Q;
+    bool has_q = false, dplr = false;
+    int qk = 0;
+    DevBuf<int> perm, row_of, q_row_of;
+    DevBuf<double> c, l, u, lo, hi, R, C, Rres, Cres;  // scaled FP64 data
+    DevBuf<double> F64, D64;                            // scaled DPLR factor
+    DevBuf<double> scal;  // 0 bscale 1 cscale 2 normA 3 normQ 4 bnorm 5 cnorm 6 w0 7..9 power scratch
+    DevBuf<double> red_partials;
+    DevBuf<double> x64, y64, xr64, yr64, xo, yo;
+    DevBuf<double> work1, work2;  // n / m FP64 scratch
+    VecSet<float> v32;
+    VecSet<double> v64;
+    DevBuf<SolveState> st;
+    SolveState* st_host = nullptr;  // pinned mirror
+    DevBuf<double> partials;
+    std::unique_ptr<LevelGraph> graphs[3];
+    double scal_host[10] = {};
+    double setup_seconds = 0.0;
+    long long launches = 0;  // kernel launches of the last solve
+    bool solved = false;
+
+    ~Problem() {
+        for (auto& g : graphs) g.reset();
+        if (st_host) cudaFreeHost(st_host);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+}  // namespace gb

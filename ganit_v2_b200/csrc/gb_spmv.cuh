@@ -1,0 +1,238 @@
+// CSR SpMV with a fused per-row epilogue, scheduled by row blocks.
+//
+// Method: CSR-Adaptive (Greathouse & Daga, SC'14).  At upload time the rows
+// of a matrix are cut, from its row-length histogram, into blocks:
+//   * STREAM  consecutive rows whose nonzeros total <= kBlockNnz and whose
+//             count <= kThreads.  The CTA streams the block's contiguous
+//             idx/val range with coalesced loads, stages the products
+//             val*x[idx] in shared memory, then reduces each row with a group
+//             of G lanes (G = power of two chosen from the rows per block).
+//   * LONG    one row with more than kBlockNnz nonzeros, reduced by the whole
+//             CTA (<= kLongSingle nonzeros) or
+//   * CHUNK   a slice of a very long row: each CTA writes its partial sum to a
+//             fixed slot and the last CTA to arrive adds the slots in chunk
+//             order and runs the epilogue (no spin-waits, deterministic).
+// Every row is reduced in a fixed order, so results are bit-reproducible run
+// to run.  One CTA per block; the epilogue functor receives (row, sums) once
+// per row, which is what lets the PDHG steps fuse into the product kernels.
+#pragma once
+#include "gb_common.cuh"
+
+namespace gb {
+
+constexpr int kBlockNnz = 2048;     // nonzeros per STREAM block
+constexpr int kLongSingle = 16384;  // longest row one CTA reduces alone
+constexpr int kChunkNnz = 8192;     // slice of a longer row per CTA
+
+enum BlockKind : int { kStream = 0, kLong = 1, kChunk = 2 };
+
+struct alignas(16) RowBlock {
+    int r0, r1;         // rows [r0, r1)
+    int p0, p1;         // nonzeros [p0, p1)
+    int kind, lg;       // BlockKind, log2 of the group size (STREAM)
+    int chunk, nchunks; // CHUNK: index and count
+    int slot_base;      // CHUNK: first slot of the row
+    int counter;        // CHUNK: arrival counter of the row
+    int pad0, pad1;
+};
+
+// Host: row-length-driven schedule.  `block_nnz` / `max_rows` are the
+// tunables (the batch autotuner varies them).
+struct Schedule {
+    std::vector<RowBlock> blocks;
+    int nslots = 0, ncounters = 0;
+    int max_lg = 0;
+};
+
+inline int floor_log2(int v) {
+    int l = 0;
+    while ((2 << l) <= v) ++l;
+    return l;
+}
+
+inline Schedule build_schedule(const int* ptr, int rows, int block_nnz = kBlockNnz, int max_rows = kThreads) {
+    Schedule s;
+    int i = 0;
+    while (i < rows) {
+        const int len = ptr[i + 1] - ptr[i];
+        if (len > block_nnz) {
+            if (len <= kLongSingle) {
+                RowBlock b{};
+                b.r0 = i; b.r1 = i + 1; b.p0 = ptr[i]; b.p1 = ptr[i + 1]; b.kind = kLong;
+                s.blocks.push_back(b);
+            } else {
+                const int nch = div_up(len, kChunkNnz);
+                for (int c = 0; c < nch; ++c) {
+                    RowBlock b{};
+                    b.r0 = i; b.r1 = i + 1;
+                    b.p0 = ptr[i] + c * kChunkNnz;
+                    b.p1 = std::min(ptr[i + 1], b.p0 + kChunkNnz);
+                    b.kind = kChunk; b.chunk = c; b.nchunks = nch;
+                    b.slot_base = s.nslots; b.counter = s.ncounters;
+                    s.blocks.push_back(b);
+                }
+                s.nslots += nch;
+                s.ncounters += 1;
+            }
+            ++i;
+            continue;
+        }
+        const int r0 = i, start = ptr[i];
+        while (i < rows && (i - r0) < max_rows && ptr[i + 1] - start <= block_nnz) ++i;
+        RowBlock b{};
+        b.r0 = r0; b.r1 = i; b.p0 = start; b.p1 = ptr[i]; b.kind = kStream;
+        const int nrows = i - r0;
+        int g = kThreads / nrows;  // lanes available per row
+        if (g > 32) g = 32;
+        b.lg = floor_log2(g < 1 ? 1 : g);
+        s.max_lg = std::max(s.max_lg, b.lg);
+        s.blocks.push_back(b);
+    }
+    return s;
+}
+
+// Device-resident schedule of one matrix.
+struct DevSchedule {
+    DevBuf<RowBlock> blocks;
+    DevBuf<double> slots;
+    DevBuf<unsigned> counters;
+    int nb = 0;
+    int nslots = 0;
+    void upload(const Schedule& s, int nv_max, cudaStream_t st) {
+        nb = static_cast<int>(s.blocks.size());
+        blocks.reset(nb ? nb : 1);
+        blocks.upload(s.blocks.data(), nb, st);
+        nslots = s.nslots;
+        slots.reset(static_cast<size_t>(s.nslots ? s.nslots : 1) * nv_max);
+        counters.reset(s.ncounters ? s.ncounters : 1);
+        GB_CUDA(cudaMemsetAsync(counters.get(), 0, counters.size() * sizeof(unsigned), st));
+    }
+};
+
+// Raw view of a CSR matrix on the device.
+template <class M>
+struct CsrView {
+    const int* __restrict__ ptr;
+    const int* __restrict__ idx;
+    const M* __restrict__ val;
+    const RowBlock* __restrict__ blocks;
+    double* slots;
+    unsigned* counters;
+    int rows;
+    int nb;
+};
+
+// Gather of a single right-hand side.
+template <class V>
+struct GatherOne {
+    const V* __restrict__ v;
+    __device__ __forceinline__ void operator()(int j, V (&o)[1]) const { o[0] = __ldg(v + j); }
+};
+
+// Shared memory needed by spmv_block for NV vectors of type V.
+template <int NV, class V>
+constexpr size_t spmv_smem_bytes() {
+    return sizeof(V) * NV * kBlockNnz + sizeof(double) * kWarps * NV + 64;
+}
+
+// Process one block.  Gather g(col, V(&)[NV]) supplies the NV vector values of
+// a column; epi(row, const V(&)[NV]) consumes a finished row.  `smem` is the
+// dynamic shared memory of spmv_smem_bytes<NV,V>().
+template <int NV, class M, class V, class Gather, class Epi>
+__device__ __forceinline__ void spmv_block(const CsrView<M>& A, const RowBlock& b, const Gather& g, Epi& epi,
+                                           unsigned char* smem) {
+    V* prod = reinterpret_cast<V*>(smem);
+    const int tid = threadIdx.x;
+    if (b.kind == kStream) {
+        const int cnt = b.p1 - b.p0;
+        // 1) coalesced stream over the block's nonzeros, products to shared memory
+#pragma unroll 4
+        for (int k = tid; k < cnt; k += kThreads) {
+            const int p = b.p0 + k;
+            const int j = __ldg(A.idx + p);
+            const V a = static_cast<V>(__ldg(A.val + p));
+            V xv[NV];
+            g(j, xv);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) prod[v * kBlockNnz + k] = a * xv[v];
+        }
+        __syncthreads();
+        // 2) each row reduced by a group of G lanes, fixed order
+        const int lg = b.lg, G = 1 << lg;
+        const int lane_g = tid & (G - 1), grp = tid >> lg;
+        const int nrows = b.r1 - b.r0;
+        for (int base = 0; base < nrows; base += (kThreads >> lg)) {
+            const int rr = base + grp;
+            const bool act = rr < nrows;
+            V acc[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) acc[v] = V(0);
+            if (act) {
+                const int r = b.r0 + rr;
+                const int s = __ldg(A.ptr + r) - b.p0, e = __ldg(A.ptr + r + 1) - b.p0;
+                for (int k = s + lane_g; k < e; k += G) {
+#pragma unroll
+                    for (int v = 0; v < NV; ++v) acc[v] += prod[v * kBlockNnz + k];
+                }
+            }
+            for (int o = G >> 1; o > 0; o >>= 1) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) acc[v] += __shfl_down_sync(0xffffffffu, acc[v], o, G);
+            }
+            if (act && lane_g == 0) epi(b.r0 + rr, acc);
+        }
+        return;
+    }
+    // LONG / CHUNK: whole CTA strides over the slice, block reduction.
+    V acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[v] = V(0);
+    for (int p = b.p0 + tid; p < b.p1; p += kThreads) {
+        const int j = __ldg(A.idx + p);
+        const V a = static_cast<V>(__ldg(A.val + p));
+        V xv[NV];
+        g(j, xv);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) acc[v] += a * xv[v];
+    }
+    V* red = reinterpret_cast<V*>(smem + sizeof(V) * NV * kBlockNnz);
+    const int lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        V t = warp_sum(acc[v]);
+        if (lane == 0) red[wid * NV + v] = t;
+    }
+    __syncthreads();
+    if (tid == 0) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            V t = V(0);
+            for (int w = 0; w < kWarps; ++w) t += red[w * NV + v];
+            acc[v] = t;
+        }
+        if (b.kind == kLong) {
+            epi(b.r0, acc);
+        } else {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) A.slots[static_cast<size_t>(b.slot_base + b.chunk) * NV + v] = double(acc[v]);
+            __threadfence();
+            const unsigned prev = atomicAdd(A.counters + b.counter, 1u);
+            if (prev == static_cast<unsigned>(b.nchunks - 1)) {
+                __threadfence();
+                V tot[NV];
+#pragma unroll
+                for (int v = 0; v < NV; ++v) tot[v] = V(0);
+                for (int c = 0; c < b.nchunks; ++c) {
+#pragma unroll
+                    for (int v = 0; v < NV; ++v)
+                        tot[v] += static_cast<V>(__ldcg(A.slots + static_cast<size_t>(b.slot_base + c) * NV + v));
+                }
+                A.counters[b.counter] = 0u;  // re-armed for the next launch (stream order)
+                epi(b.r0, tot);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+}  // namespace gb

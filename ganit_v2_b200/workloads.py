@@ -51,7 +51,8 @@ def _distinct_rows(rng, n_cols: int, m: int, k_per_col: np.ndarray) -> tuple[np.
 
 
 def random_feasible_lp(m: int = 2000, n: int = 5000, nnz_per_col=8, seed: int = 0, ub: float = 10.0,
-                       eq_frac: float = 0.5, bound_frac: float = 0.3, name: str | None = None) -> LP:
+                       eq_frac: float = 0.5, bound_frac: float = 0.3, name: str | None = None,
+                       free_frac: float = 0.0) -> LP:
     """Feasible-by-construction random LP.
 
     Rows ``[0, m*eq_frac)`` are equalities, the rest ``<=`` rows.  Columns are
@@ -60,7 +61,9 @@ def random_feasible_lp(m: int = 2000, n: int = 5000, nnz_per_col=8, seed: int = 
     ``U(0,1)`` slack on ``<=`` rows).  A dual point ``y0 ~ N(0,1)`` (``<= 0`` on
     ``<=`` rows) and reduced costs ``s0`` complementary to ``x0`` give
     ``c = A^T y0 + s0``.  ``nnz_per_col`` is an int or an array of per-column
-    counts.
+    counts.  ``free_frac`` of the columns (drawn after everything else, so
+    the default stream is unchanged) become free (-inf, +inf) with zero
+    reduced cost, which keeps the LP bounded.
     """
     rng = np.random.default_rng(seed)
     k = np.full(n, nnz_per_col, dtype=np.int64) if np.isscalar(nnz_per_col) else np.asarray(nnz_per_col)
@@ -93,7 +96,14 @@ def random_feasible_lp(m: int = 2000, n: int = 5000, nnz_per_col=8, seed: int = 
     hi = b.copy()
     lo[:n_eq] = b[:n_eq]
     lo[n_eq:] = -np.inf
-    return LP(Csr.from_scipy(A), c, np.zeros(n), np.full(n, ub), lo, hi,
+    l = np.zeros(n)
+    u = np.full(n, ub)
+    if free_frac > 0:
+        free = (rng.random(n) < free_frac) & ~at_bound
+        l[free] = -np.inf
+        u[free] = np.inf
+        c = c - s0 * free  # s0 is already 0 there; kept explicit
+    return LP(Csr.from_scipy(A), c, l, u, lo, hi,
               name=name or f"rand_m{m}_n{n}_s{seed}", meta={"x0": x0, "y0": y0})
 
 

@@ -1,0 +1,244 @@
+/*
+ * ganit_b200.h -- C ABI of the B200-native restarted-PDHG engine (LP + convex QP).
+ *
+ * Library: ganit_v2_b200/libganit_b200.so (sm_100a).  Every function returns
+ * an int status (GB_OK == 0, negative on error) and never throws; the message
+ * of the last error on the calling thread is gb_last_error().  Handles are
+ * bound to one CUDA device and one stream and are not thread-safe; the caller
+ * owns every host buffer, the library owns every device buffer.
+ *
+ * Three layers, each replacing one reference interface (paths inside the
+ * GANIT_v2 project):
+ *
+ *  1. Fused solver      gb_solve / gb_problem_*        replaces
+ *       ganit::solve_pdhg_gpu(const LP&, const Options&)  include/ganit/pdhg.hpp:44-47,
+ *       i.e. run_pdhg<CudaBackend...> (src/pdhg_impl.hpp:243-328, src/backend_cuda.cu:382-393).
+ *       Scaling, the PDHG iteration, KKT checks, restarts, primal weight,
+ *       infeasibility test, precision phases and FP64 certification all run
+ *       on the device; one CUDA-graph launch per precision phase.
+ *
+ *  2. Backend ops       gb_backend_* / gb_vec_* / gb_spmv_* ...  replace the
+ *       compile-time Backend concept that pdhg_impl.hpp drives (implemented by
+ *       CudaBackend<M,V>, src/backend_cuda.cu:286-378).  A thin C++ adapter
+ *       (include/ganit_b200_backend.hpp) satisfies that concept with these
+ *       calls, so run_pdhg can drive the B200 kernels unchanged.
+ *
+ *  3. Batched and differentiable solving  gb_batch_* / gb_diff_*  (no
+ *       counterpart in the reference; README.md:196 lists batched GPU solving
+ *       as planned).
+ */
+#ifndef GANIT_B200_H
+#define GANIT_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes */
+enum {
+    GB_OK = 0,
+    GB_ERR_INVALID = -1,   /* bad argument or malformed problem */
+    GB_ERR_CUDA = -2,      /* CUDA runtime error (message in gb_last_error) */
+    GB_ERR_NOMEM = -3,     /* device allocation failed */
+    GB_ERR_NODEVICE = -4,  /* no sm_100 device visible */
+    GB_ERR_UNSUPPORTED = -5
+};
+
+/* ---- solver status, include/ganit/pdhg.hpp:27 (same order) */
+enum { GB_OPTIMAL = 0, GB_PRIMAL_INFEASIBLE = 1, GB_ITERATION_LIMIT = 2, GB_TIME_LIMIT = 3, GB_NUMERICAL_ERROR = 4 };
+
+/* ---- precision schedule, include/ganit/pdhg.hpp:10 (same order) */
+enum { GB_PREC_DOUBLE = 0, GB_PREC_MIXED = 1, GB_PREC_DYNAMIC = 2 };
+
+/* ---- value types for gb_backend_create */
+enum { GB_F32 = 0, GB_F64 = 1 };
+
+/* Problem in GANIT's form (include/ganit/lp.hpp:4-47):
+ *   minimise c'x + 0.5 x'Qx + obj_const  s.t.  lo <= A x <= hi,  l <= x <= u.
+ * A is host CSR (int32 ptr[m+1], idx[nnz], double val[nnz]); bounds may be
+ * +-INFINITY.  Q is either a full-storage symmetric CSR (q_ptr != NULL, as in
+ * the reference) or diagonal-plus-low-rank Q = 2 (F F^T + diag(D)) with F an
+ * n x q_rank row-major host array (q_rank > 0), or absent. */
+typedef struct {
+    int32_t m, n;
+    const int32_t* a_ptr;
+    const int32_t* a_idx;
+    const double* a_val;
+    const double* c;
+    const double* l;
+    const double* u;
+    const double* lo;
+    const double* hi;
+    double obj_const;
+    int32_t maximize;
+    const int32_t* q_ptr;
+    const int32_t* q_idx;
+    const double* q_val;
+    int32_t q_rank;
+    const double* q_F;
+    const double* q_D;
+} gb_lp;
+
+/* ganit::Options (include/ganit/pdhg.hpp:12-25), same meaning and defaults. */
+typedef struct {
+    double tol;              /* 1e-4 relative KKT tolerance */
+    int64_t max_iter;        /* 10000000 */
+    double time_limit;       /* 3600 s */
+    int32_t check_every;     /* 64 */
+    int32_t ruiz_iters;      /* 10 */
+    int32_t pock_chambolle;  /* 1 */
+    double infeas_tol;       /* 1e-8 */
+    int32_t precision;       /* GB_PREC_DOUBLE */
+    int32_t stall_checks;    /* 12 */
+    int32_t stall_checks_l2; /* 24 */
+    int32_t verbose;         /* 0 (the engine prints nothing) */
+} gb_options;
+
+/* ganit::Result (include/ganit/pdhg.hpp:30-42) without the vectors, which go
+ * to caller buffers; plus engine diagnostics. */
+typedef struct {
+    int32_t status;
+    double pobj, dobj;
+    double rel_primal, rel_dual, rel_gap;
+    int64_t iterations, fp32_iterations, l2_iterations;
+    int32_t restarts;
+    double setup_seconds, solve_seconds;
+    double norm_a;        /* ||A'||_2 estimate of the scaled matrix */
+    double primal_weight; /* final primal weight w */
+    int32_t checks;       /* KKT checks performed */
+    int32_t phases;       /* precision phases run */
+} gb_result;
+
+/* ---------------------------------------------------------------- common */
+const char* gb_last_error(void);
+int gb_version(void);                       /* 10000*major + 100*minor + patch */
+void gb_default_options(gb_options* opt);
+/* Selects the CUDA device used by handles created afterwards on this thread. */
+int gb_set_device(int device);
+
+/* ---------------------------------------------------------------- 1. fused solver */
+/* One-shot solve of a host problem: upload, scale (on the device), restarted
+ * PDHG with the precision schedule of opt, FP64 certification, unscale,
+ * download.  x_out[n] / y_out[m] may be NULL.  Same contract as
+ * ganit::solve_pdhg_gpu (include/ganit/pdhg.hpp:44-47). */
+int gb_solve(const gb_lp* lp, const gb_options* opt, gb_result* res, double* x_out, double* y_out);
+
+typedef struct gb_problem gb_problem;
+/* Upload + scale once (scaling options taken from opt: ruiz_iters,
+ * pock_chambolle); the scaled problem stays resident in HBM. */
+int gb_problem_create(const gb_lp* lp, const gb_options* opt, gb_problem** out);
+/* Solve the resident problem from the default start (x0 = proj(0), y0 = 0).
+ * Results stay on the device until gb_problem_get_solution. */
+int gb_problem_solve(gb_problem* p, const gb_options* opt, gb_result* res);
+/* Copy the unscaled solution of the last solve to host buffers (either may be NULL). */
+int gb_problem_get_solution(gb_problem* p, double* x_out, double* y_out);
+void gb_problem_destroy(gb_problem* p);
+/* Stream the problem's work is issued on (a cudaStream_t). */
+void* gb_problem_stream(gb_problem* p);
+/* Kernel-level timing of one precision level (0 = L1, 1 = L2, 2 = L3):
+ * runs `iters` plain PDHG iterations from the current iterate with CUDA
+ * events around every launch and reports the mean duration (ms) of the fused
+ * primal kernel (A^T y + primal step) and of the fused dual kernel (A xbar +
+ * dual step), and the number of launches issued. */
+int gb_problem_time_kernels(gb_problem* p, int level, int iters, double* ms_primal, double* ms_dual,
+                            int64_t* launches);
+/* Counters of the last gb_problem_solve: kernel launches issued inside the
+ * solve, and algorithmic bytes moved by the fused iteration kernels per
+ * iteration at each level (index 0..2 = L1..L3). */
+int gb_problem_stats(gb_problem* p, int64_t* launches, double* bytes_per_iter_level);
+
+/* ---------------------------------------------------------------- 2. backend ops
+ * Mirrors the Backend concept used at src/pdhg_impl.hpp:73-84, 92-118,
+ * 133-137, 145-146, 178-194, 207-220.  The problem passed to
+ * gb_backend_create is already SCALED (ganit::ScaledLP, src/scaling.hpp:8-23):
+ * A and its stored transpose AT, optional CSR Q, and the scaled vectors. */
+typedef struct {
+    int32_t m, n;
+    const int32_t* a_ptr; const int32_t* a_idx; const double* a_val;
+    const int32_t* at_ptr; const int32_t* at_idx; const double* at_val;
+    const int32_t* q_ptr; const int32_t* q_idx; const double* q_val; /* NULL for LP */
+    const double *c, *l, *u, *lo, *hi, *rres, *cres;
+} gb_scaled_lp;
+
+typedef struct gb_backend gb_backend;
+typedef struct gb_vec gb_vec;
+
+/* CudaBackend<M,V>(const ScaledLP&) (backend_cuda.cu:294-303); mat_type and
+ * vec_type are GB_F32 / GB_F64. */
+int gb_backend_create(const gb_scaled_lp* s, int mat_type, int vec_type, gb_backend** out);
+void gb_backend_destroy(gb_backend* b);
+/* zeros(k) (backend_cuda.cu:305) */
+int gb_vec_zeros(gb_backend* b, int k, gb_vec** out);
+/* from_host(h) (backend_cuda.cu:306) */
+int gb_vec_from_host(gb_backend* b, const double* h, int k, gb_vec** out);
+/* to_host(v) (backend_cuda.cu:307-315); h must hold gb_vec_size(v) doubles */
+int gb_vec_to_host(gb_backend* b, const gb_vec* v, double* h);
+int gb_vec_size(const gb_vec* v);
+void gb_vec_destroy(gb_vec* v);
+/* copy / fill (backend_cuda.cu:316-322) */
+int gb_copy(gb_backend* b, const gb_vec* src, gb_vec* dst);
+int gb_fill(gb_backend* b, gb_vec* v, double a);
+/* spmv_A / spmv_AT / spmv_Q (backend_cuda.cu:324-335) */
+int gb_spmv_A(gb_backend* b, const gb_vec* x, gb_vec* ax);
+int gb_spmv_AT(gb_backend* b, const gb_vec* y, gb_vec* aty);
+int gb_spmv_Q(gb_backend* b, const gb_vec* x, gb_vec* qx);
+/* primal_step / dual_step (backend_cuda.cu:337-344); qx may be NULL */
+int gb_primal_step(gb_backend* b, const gb_vec* x, const gb_vec* aty, const gb_vec* qx, double tau, gb_vec* xn,
+                   gb_vec* xbar, gb_vec* sumx);
+int gb_dual_step(gb_backend* b, const gb_vec* y, const gb_vec* axbar, double sigma, gb_vec* yn, gb_vec* sumy);
+/* sub / scale_into (backend_cuda.cu:345-350) */
+int gb_sub(gb_backend* b, const gb_vec* a, const gb_vec* c, gb_vec* d);
+int gb_scale_into(gb_backend* b, const gb_vec* src, double a, gb_vec* dst);
+/* FP64-accumulated reductions (backend_cuda.cu:363-377), results to host */
+int gb_primal_res2(gb_backend* b, const gb_vec* ax, double* out);
+int gb_dual_res(gb_backend* b, const gb_vec* aty, const gb_vec* qx, int with_c, double* rd2, double* vobj);
+int gb_row_dual_obj(gb_backend* b, const gb_vec* y, double* out);
+int gb_dot(gb_backend* b, const gb_vec* a, const gb_vec* c, double* out);
+int gb_dot_c(gb_backend* b, const gb_vec* x, double* out);
+int gb_diff2(gb_backend* b, const gb_vec* a, const gb_vec* c, double* out);
+
+/* ---------------------------------------------------------------- 3a. batched solving
+ * Many independent LPs (no Q) solved by ONE persistent kernel: each thread
+ * block owns one instance at a time (largest first) and runs the whole
+ * restarted PDHG for it -- iterations, KKT checks, restarts, primal weight,
+ * infeasibility test, FP32 phase then FP64 finish -- with block-level
+ * synchronisation only.  opt->precision: GB_PREC_DOUBLE (FP64 throughout) or
+ * GB_PREC_MIXED (FP32 matrix + iterates, FP64 finish); every result is
+ * certified in FP64. */
+typedef struct gb_batch gb_batch;
+int gb_batch_create(int count, const gb_lp* lps, const gb_options* opt, gb_batch** out);
+/* Solve every instance; results[count] receives per-instance results. */
+int gb_batch_solve(gb_batch* b, const gb_options* opt, gb_result* results);
+/* Unscaled solution of instance i (either buffer may be NULL). */
+int gb_batch_get_solution(gb_batch* b, int i, double* x_out, double* y_out);
+/* Schedule chosen by the autotuner: threads per block, blocks per SM, and
+ * the row-split group sizes picked per instance (written to groups[count*2]
+ * when groups != NULL: group size for A rows, for A^T rows). */
+int gb_batch_schedule(gb_batch* b, int* threads, int* blocks_per_sm, int* groups);
+void gb_batch_destroy(gb_batch* b);
+
+/* ---------------------------------------------------------------- 3b. differentiable solving
+ * Forward: restarted PDHG to opt->tol on every instance of a batch, then
+ * `tail_iters` (K) plain PDHG iterations in FP64 with fixed steps, storing a
+ * checkpoint of (x, y) every `ckpt_every` (R) iterations; the outputs are the
+ * last tail iterate (x*, y*) in original units.
+ * Backward: given dL/dx* and dL/dy*, reverse-mode through the K tail
+ * iterations (recomputing each R-segment from its checkpoint) and the
+ * scaling, returning dL/dc, dL/dlo, dL/dhi and dL/d(A values) (CSR order of
+ * the input A) in original units. */
+typedef struct gb_diff gb_diff;
+int gb_diff_create(int count, const gb_lp* lps, const gb_options* opt, int tail_iters, int ckpt_every,
+                   gb_diff** out);
+/* x_out: concatenation of the instances' x (sum n), y_out: of y (sum m). */
+int gb_diff_forward(gb_diff* d, const gb_options* opt, gb_result* results, double* x_out, double* y_out);
+/* dl_dx (sum n), dl_dy (sum m) in; dl_dc (sum n), dl_dlo / dl_dhi (sum m),
+ * dl_dval (sum nnz) out.  Any output may be NULL. */
+int gb_diff_backward(gb_diff* d, const double* dl_dx, const double* dl_dy, double* dl_dc, double* dl_dlo,
+                     double* dl_dhi, double* dl_dval);
+void gb_diff_destroy(gb_diff* d);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GANIT_B200_H */

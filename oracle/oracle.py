@@ -132,6 +132,7 @@ def solve(lp, **opts) -> OracleResult:
     x = np.zeros(lp.n)
     y = np.zeros(lp.m)
     lib.ora_solve_pdhg.restype = C.c_int
+    lib.ora_solve_pdhg.argtypes = [C.c_void_p] * 5
     rc = lib.ora_solve_pdhg(C.byref(s), C.byref(o), C.byref(r), _p(x), _p(y))
     if rc != 0:
         raise RuntimeError(f"ora_solve_pdhg failed ({rc})")
@@ -151,6 +152,8 @@ def scale(lp, ruiz_iters=10, pock_chambolle=True) -> dict:
     out.update({k: np.zeros(m) for k in ("lo", "hi", "R", "Rres")})
     out["a_val"] = np.zeros(lp.A.nnz)
     scal = np.zeros(7)
+    lib.ora_scale.restype = C.c_int
+    lib.ora_scale.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 11
     rc = lib.ora_scale(C.byref(s), int(ruiz_iters), int(pock_chambolle), _p(out["a_val"]), _p(out["c"]),
                        _p(out["l"]), _p(out["u"]), _p(out["lo"]), _p(out["hi"]), _p(out["R"]), _p(out["C"]),
                        _p(out["Rres"]), _p(out["Cres"]), _p(scal))

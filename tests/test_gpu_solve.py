@@ -1,0 +1,99 @@
+"""Parity of the fused B200 solver (gb_solve through the C ABI) with the
+reference CPU PDHG, on the golden fixtures the reference produced.
+
+Bar (the engine's tolerance statement): same verdict; every OPTIMAL result
+FP64-certified within tol (rel_p, rel_d, rel_gap <= tol); objective within
+10 * tol relative of the reference's; at FP64 the trajectory matches the
+reference's iteration count to within two KKT checks."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from tests.golden.make_golden import load_lp
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+with open(os.path.join(GOLD, "golden.json")) as f:
+    GOLDEN = json.load(f)
+
+PREC = {"double": 0, "mixed": 1, "dynamic": 2}
+
+
+@pytest.fixture(scope="module")
+def gb():
+    import ganit_v2_b200 as gb
+
+    gb.load_library()
+    return gb
+
+
+def check_against(r, g, tol, prec, check_every=64):
+    assert r.status_name == g["status"]
+    if g["status"] == "OPTIMAL":
+        assert r.rel_primal <= tol * 1.0000001 and r.rel_dual <= tol * 1.0000001 and r.rel_gap <= tol * 1.0000001
+        assert abs(r.pobj - g["pobj"]) <= 10 * tol * (1 + abs(g["pobj"])), (r.pobj, g["pobj"])
+        assert abs(r.dobj - g["dobj"]) <= 10 * tol * (1 + abs(g["dobj"])), (r.dobj, g["dobj"])
+    if prec == "double":
+        assert abs(r.iterations - g["iterations"]) <= 2 * check_every, (r.iterations, g["iterations"])
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN["synthetic"]))
+@pytest.mark.parametrize("prec", ["double", "mixed", "dynamic"])
+def test_solve_matches_reference(gb, name, prec):
+    lp, arr = load_lp(os.path.join(GOLD, name + ".npz"))
+    entry = GOLDEN["synthetic"][name]
+    tol = entry["options"].get("tol", 1e-4)
+    r = gb.solve_pdhg_gpu(lp, gb.Options(tol=tol, precision=gb.Precision(PREC[prec])))
+    check_against(r, entry["results"][prec], tol, prec)
+    assert r.x.shape == (lp.n,) and r.y.shape == (lp.m,)
+    assert np.all(np.isfinite(r.x)) and np.all(np.isfinite(r.y))
+    if prec == "double" and entry["results"][prec]["status"] == "OPTIMAL":
+        xr = arr["x_double"]
+        assert np.linalg.norm(r.x - xr) <= 1e-3 * (1 + np.linalg.norm(xr))
+
+
+def test_resident_problem_repeats_bit_identically(gb):
+    lp, _ = load_lp(os.path.join(GOLD, "rand_cfg0.npz"))
+    with gb.Problem(lp) as p:
+        r1 = p.solve(gb.Options(precision=gb.Precision.Mixed))
+        r2 = p.solve(gb.Options(precision=gb.Precision.Mixed))
+    assert r1.iterations == r2.iterations and r1.pobj == r2.pobj
+    np.testing.assert_array_equal(r1.x, r2.x)
+    np.testing.assert_array_equal(r1.y, r2.y)
+
+
+def test_iteration_limit_and_check_every(gb):
+    lp, _ = load_lp(os.path.join(GOLD, "rand_small.npz"))
+    r = gb.solve_pdhg_gpu(lp, gb.Options(max_iter=100, check_every=50))
+    assert r.status == gb.Status.IterationLimit and r.iterations == 100
+    r = gb.solve_pdhg_gpu(lp, gb.Options(check_every=33))
+    assert r.status == gb.Status.Optimal and r.iterations % 33 == 0
+
+
+def test_odd_check_every_matches_oracle(gb, oracle_built):
+    lp, _ = load_lp(os.path.join(GOLD, "rand_small.npz"))
+    o = oracle_built.solve(lp, check_every=37)
+    r = gb.solve_pdhg_gpu(lp, gb.Options(check_every=37))
+    assert r.status_name == o.status
+    assert abs(r.iterations - o.iterations) <= 74
+    assert abs(r.pobj - o.pobj) <= 1e-3 * (1 + abs(o.pobj))
+
+
+def test_time_limit_reported(gb):
+    lp, _ = load_lp(os.path.join(GOLD, "rand_tight.npz"))
+    r = gb.solve_pdhg_gpu(lp, gb.Options(tol=1e-12, time_limit=0.0))
+    assert r.status == gb.Status.TimeLimit
+
+
+def test_invalid_problem_is_an_error_not_a_crash(gb):
+    lp, _ = load_lp(os.path.join(GOLD, "rand_small.npz"))
+    bad = gb.LP(gb.Csr(lp.m, lp.n, lp.A.ptr, np.where(lp.A.idx > 5, lp.n + 7, lp.A.idx), lp.A.val), lp.c, lp.l,
+                lp.u, lp.lo, lp.hi)
+    with pytest.raises(gb.GanitError) as e:
+        gb.solve_pdhg_gpu(bad)
+    assert e.value.code == -1 and "out of range" in str(e.value)
+    nan = gb.LP(lp.A, np.full(lp.n, np.nan), lp.l, lp.u, lp.lo, lp.hi)
+    r = gb.solve_pdhg_gpu(nan, gb.Options(max_iter=640))
+    assert r.status in (gb.Status.NumericalError, gb.Status.IterationLimit)
