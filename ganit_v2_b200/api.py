@@ -124,6 +124,15 @@ class _GbScaledLp(C.Structure):
                                   "c", "l", "u", "lo", "hi", "rres", "cres")]
 
 
+class GbKktScalars(C.Structure):
+    _fields_ = [("obj_scale", C.c_double), ("obj_const", C.c_double), ("bnorm", C.c_double), ("cnorm", C.c_double)]
+
+
+class GbKkt(C.Structure):
+    _fields_ = [("pobj", C.c_double), ("dobj", C.c_double), ("rel_p", C.c_double), ("rel_d", C.c_double),
+                ("rel_gap", C.c_double), ("err", C.c_double)]
+
+
 # Every symbol of include/ganit_b200.h (checked by the tests).
 EXPORTS = [
     "gb_last_error", "gb_version", "gb_default_options", "gb_set_device", "gb_solve", "gb_problem_create",
@@ -133,7 +142,7 @@ EXPORTS = [
     "gb_spmv_AT", "gb_spmv_Q", "gb_primal_step", "gb_dual_step", "gb_sub", "gb_scale_into", "gb_primal_res2",
     "gb_dual_res", "gb_row_dual_obj", "gb_dot", "gb_dot_c", "gb_diff2", "gb_batch_create", "gb_batch_solve",
     "gb_batch_get_solution", "gb_batch_schedule", "gb_batch_destroy", "gb_diff_create", "gb_diff_forward",
-    "gb_diff_backward", "gb_diff_destroy",
+    "gb_diff_backward", "gb_diff_destroy", "gb_eval_kkt_noalloc",
 ]
 
 _lib = None
@@ -169,6 +178,7 @@ def load_library(path: str = LIB_PATH):
         "gb_batch_destroy": (None, [vp]), "gb_diff_create": (i32, [i32, vp, vp, i32, i32, vp]),
         "gb_diff_forward": (i32, [vp, vp, vp, vp, vp]),
         "gb_diff_backward": (i32, [vp, vp, vp, vp, vp, vp, vp]), "gb_diff_destroy": (None, [vp]),
+        "gb_eval_kkt_noalloc": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

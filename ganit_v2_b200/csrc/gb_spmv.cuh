@@ -50,8 +50,11 @@ inline int floor_log2(int v) {
     return l;
 }
 
-inline Schedule build_schedule(const int* ptr, int rows, int block_nnz = kBlockNnz, int max_rows = kThreads) {
-    Schedule s;
+// Walks the rows once and hands every block to `emit`; slot and counter ids
+// are numbered from *nslots / *ncounters on.
+template <class Emit>
+inline void schedule_rows(const int* ptr, int rows, int block_nnz, int max_rows, int* nslots, int* ncounters,
+                          Emit&& emit) {
     int i = 0;
     while (i < rows) {
         const int len = ptr[i + 1] - ptr[i];
@@ -59,7 +62,7 @@ inline Schedule build_schedule(const int* ptr, int rows, int block_nnz = kBlockN
             if (len <= kLongSingle) {
                 RowBlock b{};
                 b.r0 = i; b.r1 = i + 1; b.p0 = ptr[i]; b.p1 = ptr[i + 1]; b.kind = kLong;
-                s.blocks.push_back(b);
+                emit(b);
             } else {
                 const int nch = div_up(len, kChunkNnz);
                 for (int c = 0; c < nch; ++c) {
@@ -68,11 +71,11 @@ inline Schedule build_schedule(const int* ptr, int rows, int block_nnz = kBlockN
                     b.p0 = ptr[i] + c * kChunkNnz;
                     b.p1 = std::min(ptr[i + 1], b.p0 + kChunkNnz);
                     b.kind = kChunk; b.chunk = c; b.nchunks = nch;
-                    b.slot_base = s.nslots; b.counter = s.ncounters;
-                    s.blocks.push_back(b);
+                    b.slot_base = *nslots; b.counter = *ncounters;
+                    emit(b);
                 }
-                s.nslots += nch;
-                s.ncounters += 1;
+                *nslots += nch;
+                *ncounters += 1;
             }
             ++i;
             continue;
@@ -85,9 +88,16 @@ inline Schedule build_schedule(const int* ptr, int rows, int block_nnz = kBlockN
         int g = kThreads / nrows;  // lanes available per row
         if (g > 32) g = 32;
         b.lg = floor_log2(g < 1 ? 1 : g);
-        s.max_lg = std::max(s.max_lg, b.lg);
-        s.blocks.push_back(b);
+        emit(b);
     }
+}
+
+inline Schedule build_schedule(const int* ptr, int rows, int block_nnz = kBlockNnz, int max_rows = kThreads) {
+    Schedule s;
+    schedule_rows(ptr, rows, block_nnz, max_rows, &s.nslots, &s.ncounters, [&](const RowBlock& b) {
+        s.blocks.push_back(b);
+        s.max_lg = std::max(s.max_lg, b.lg);
+    });
     return s;
 }
 

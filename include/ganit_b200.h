@@ -198,6 +198,44 @@ int gb_dot(gb_backend* b, const gb_vec* a, const gb_vec* c, double* out);
 int gb_dot_c(gb_backend* b, const gb_vec* x, double* out);
 int gb_diff2(gb_backend* b, const gb_vec* a, const gb_vec* c, double* out);
 
+/* ---------------------------------------------------------------- KKT check without allocation
+ * No counterpart in the reference.  FP64 KKT evaluation of a point (x, y) of
+ * an already-scaled LP, for callers that cannot allocate device memory when
+ * they need a check: a branch-and-bound worker or solver service working in
+ * a fixed device-memory budget, or a latency-critical path where
+ * cudaMalloc/cudaFree would synchronise the device and stall other streams.
+ *
+ * Every pointer member of `dev` (and x[n], y[m]) points to DEVICE memory
+ * holding FP64 scaled data as in gb_scaled_lp (q_* must be NULL: LP only);
+ * h_a_ptr / h_at_ptr are HOST copies of the two row-pointer arrays.  The
+ * scalars are those of the reference's KKT formulas (pdhg_impl.hpp:92-109):
+ * obj_scale = cscale*bscale, obj_const (min-sense), and the norms bnorm and
+ * cnorm of the original right-hand side and objective.  Work runs on
+ * `stream` (a cudaStream_t, NULL = default stream) on the current device and
+ * the call returns after the result reached `out`.
+ *
+ * It calls no cudaMalloc/cudaFree and no allocating library routine: its
+ * scratch is a fixed 4 MiB __device__ array inside the library, held on every
+ * GPU that loads the library until the process exits.  Limits: at most
+ * GB_NOALLOC_MAX_BLOCKS row blocks for A and A^T together (a block is <= 2048
+ * nonzeros and <= 256 rows), GB_NOALLOC_MAX_SLOTS chunk slots and
+ * GB_NOALLOC_MAX_LONG_ROWS rows longer than 16384 nonzeros; larger problems
+ * get GB_ERR_INVALID with a message.  All calls share the array, so calls
+ * whose GPU work overlaps (unordered streams or threads) race; the first call
+ * on a device looks the array up (cudaGetSymbolAddress) and should come
+ * before any stream capture. */
+#define GB_NOALLOC_MAX_BLOCKS 16384
+#define GB_NOALLOC_MAX_SLOTS 8192
+#define GB_NOALLOC_MAX_LONG_ROWS 4096
+typedef struct {
+    double obj_scale, obj_const, bnorm, cnorm;
+} gb_kkt_scalars;
+typedef struct {  /* KKT of src/pdhg_impl.hpp:36-42 */
+    double pobj, dobj, rel_p, rel_d, rel_gap, err;
+} gb_kkt;
+int gb_eval_kkt_noalloc(const gb_scaled_lp* dev, const int32_t* h_a_ptr, const int32_t* h_at_ptr, const double* x,
+                        const double* y, const gb_kkt_scalars* sc, void* stream, gb_kkt* out);
+
 /* ---------------------------------------------------------------- 3a. batched solving
  * Many independent LPs (no Q) solved by ONE persistent kernel: each thread
  * block owns one instance at a time (largest first) and runs the whole
