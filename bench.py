@@ -184,6 +184,24 @@ def run_reference_arm(args):
     return 0
 
 
+def run_profile_case():
+    """The workload of the bench, shortened for ncu: one problem, a warm-up
+    solve and one measured solve (mixed), then 3 plain iterations per level."""
+    import ganit_v2_b200 as gb
+
+    gb.set_device(0)
+    lp = workload()
+    p = gb.Problem(lp)
+    for _ in range(2):
+        r = p.solve(gb.Options(precision=gb.Precision.Mixed), fetch=False)
+    for lvl in (0, 2):
+        p.time_kernels(lvl, 3)
+    print(json.dumps({"profile_case": WORKLOAD_DESC, "status": r.status_name, "iterations": r.iterations,
+                      "launches_per_solve": p.stats()[0]}))
+    p.close()
+    return 0
+
+
 def pinned_copy(lp):
     """Copy the LP's host arrays into page-locked memory (torch pin_memory)."""
     import torch
@@ -209,11 +227,15 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--kernel-iters", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="short fixed sequence for ncu: upload + one warm-up solve + one solve + 3 timed iterations")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.profile:
+        return run_profile_case()
 
     import torch
 

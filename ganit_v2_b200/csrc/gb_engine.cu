@@ -5,6 +5,7 @@
 // gb_backend_* / gb_vec_*  : the Backend concept ops that src/pdhg_impl.hpp
 //                            drives (replaces CudaBackend, backend_cuda.cu:286-378)
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -81,8 +82,10 @@ void upload_mat(DevMat& M, int rows, int cols, const int* ptr, const int* idx, c
     M.host_ptr.assign(ptr, ptr + rows + 1);
     M.ptr.reset(rows + 1);
     M.ptr.upload(ptr, rows + 1, s);
-    M.idx.reset(M.nnz ? M.nnz : 1);
-    M.val64.reset(M.nnz ? M.nnz : 1);
+    M.idx.reset(padded_nnz(M.nnz));
+    M.val64.reset(padded_nnz(M.nnz));
+    GB_CUDA(cudaMemsetAsync(M.idx.get(), 0, M.idx.size() * sizeof(int), s));
+    GB_CUDA(cudaMemsetAsync(M.val64.get(), 0, M.val64.size() * sizeof(double), s));
     if (M.nnz) {
         M.idx.upload(idx, M.nnz, s);
         M.val64.upload(val, M.nnz, s);
@@ -99,8 +102,10 @@ void device_transpose(Problem& P, cudaStream_t s) {
     P.row_of.reset(nnz ? nnz : 1);
     P.perm.reset(nnz ? nnz : 1);
     P.AT.ptr.reset(n + 1);
-    P.AT.idx.reset(nnz ? nnz : 1);
-    P.AT.val64.reset(nnz ? nnz : 1);
+    P.AT.idx.reset(padded_nnz(nnz));
+    P.AT.val64.reset(padded_nnz(nnz));
+    GB_CUDA(cudaMemsetAsync(P.AT.idx.get(), 0, P.AT.idx.size() * sizeof(int), s));
+    GB_CUDA(cudaMemsetAsync(P.AT.val64.get(), 0, P.AT.val64.size() * sizeof(double), s));
     const int g = elem_grid(std::max(nnz, m * 32), P.sms);
     if (m) k_row_of<<<g, kThreads, 0, s>>>(m, P.A.ptr.get(), P.row_of.get());
     DevBuf<int> cnt(n + 1), keys_out, iota;
@@ -159,10 +164,10 @@ void power_norm_A(Problem& P, cudaStream_t s) {
     reduce_to(s, n, Sq{v}, P.red_partials.get(), pw, PostSqrt{});
     k_power_step<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, v, v, pw);  // v /= ||v|| (lambda overwritten below)
     GB_CUDA(cudaMemsetAsync(pw + 1, 0, 2 * sizeof(double), s));
-    const size_t sm1 = spmv_smem_bytes<1, double>();
+    const size_t sm1 = spmv_smem_bytes_tma<1, double, double>();
     for (int it = 0; it < 50; ++it) {
-        k_spmv<double, double><<<P.A.sched.nb, kThreads, sm1, s>>>(P.A.view<double>(), v, w);
-        k_spmv<double, double><<<P.AT.sched.nb, kThreads, sm1, s>>>(P.AT.view<double>(), w, z);
+        k_spmv<double, double><<<P.A.sched.ctas(2), kThreads, sm1, s>>>(P.A.view<double>(2), v, w);
+        k_spmv<double, double><<<P.AT.sched.ctas(2), kThreads, sm1, s>>>(P.AT.view<double>(2), w, z);
         reduce_to(s, n, Sq{z}, P.red_partials.get(), pw, PostSqrt{});
         k_power_step<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, z, v, pw);
     }
@@ -181,12 +186,12 @@ void power_norm_Q(Problem& P, cudaStream_t s) {
     reduce_to(s, n, Sq{v}, P.red_partials.get(), pw, PostSqrt{});
     k_power_step<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, v, v, pw);
     GB_CUDA(cudaMemsetAsync(pw + 1, 0, 2 * sizeof(double), s));
-    const size_t sm1 = spmv_smem_bytes<1, double>();
+    const size_t sm1 = spmv_smem_bytes_tma<1, double, double>();
     for (int it = 0; it < 60; ++it) {
         if (P.dplr)
             qx_dplr_f64(P, v, w, s);
         else
-            k_spmv<double, double><<<P.Q.sched.nb, kThreads, sm1, s>>>(P.Q.view<double>(), v, w);
+            k_spmv<double, double><<<P.Q.sched.ctas(2), kThreads, sm1, s>>>(P.Q.view<double>(2), v, w);
         reduce_to(s, n, Sq{w}, P.red_partials.get(), pw, PostSqrt{});
         k_power_step<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, w, v, pw);
     }
@@ -222,30 +227,38 @@ void convert_data(Problem& P, VecSet<V>& vs, cudaStream_t s) {
     }
 }
 
+// Resident CTAs per SM of the fused iteration kernels of each precision level
+// (L1 <f,f>, L2 <f,d>, L3 <d,d>): the persistent grids are one full wave.
+int g_ctas_per_sm[kPartitions] = {4, 4, 2};
+
+template <class M, class V>
+int level_occupancy() {
+    const size_t sm = spmv_smem_bytes_tma<1, M, V>();
+    int o1 = 0, o2 = 0;
+    GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_dual<M, V>, kThreads, sm));
+    GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_primal<M, V>, kThreads, sm));
+    return std::max(1, std::min(o1, o2));
+}
+
+template <class M, class V>
+void set_level_smem() {
+    set_smem(k_spmv<M, V>, spmv_smem_bytes_tma<1, M, V>());
+    set_smem(k_primal<M, V>, spmv_smem_bytes_tma<1, M, V>());
+    set_smem(k_dual<M, V>, spmv_smem_bytes_tma<1, M, V>());
+    set_smem(k_eval<M, V, 2, 3>, spmv_smem_bytes_tma<3, M, V>());
+    set_smem(k_eval<M, V, 1, 1>, spmv_smem_bytes_tma<1, M, V>());
+    set_smem(k_spmv_q2<M, V>, spmv_smem_bytes_tma<2, M, V>());
+}
+
 void init_kernel_attrs() {
     static std::once_flag once;
     std::call_once(once, [] {
-        const size_t s1f = spmv_smem_bytes<1, float>(), s1d = spmv_smem_bytes<1, double>();
-        const size_t s3f = spmv_smem_bytes<3, float>(), s3d = spmv_smem_bytes<3, double>();
-        const size_t s2f = spmv_smem_bytes<2, float>(), s2d = spmv_smem_bytes<2, double>();
-        set_smem(k_spmv<float, float>, s1f);
-        set_smem(k_spmv<float, double>, s1d);
-        set_smem(k_spmv<double, double>, s1d);
-        set_smem(k_primal<float, float>, s1f);
-        set_smem(k_primal<float, double>, s1d);
-        set_smem(k_primal<double, double>, s1d);
-        set_smem(k_dual<float, float>, s1f);
-        set_smem(k_dual<float, double>, s1d);
-        set_smem(k_dual<double, double>, s1d);
-        set_smem(k_eval<float, float, 2, 3>, s3f);
-        set_smem(k_eval<float, double, 2, 3>, s3d);
-        set_smem(k_eval<double, double, 2, 3>, s3d);
-        set_smem(k_eval<float, float, 1, 1>, s1f);
-        set_smem(k_eval<float, double, 1, 1>, s1d);
-        set_smem(k_eval<double, double, 1, 1>, s1d);
-        set_smem(k_spmv_q2<float, float>, s2f);
-        set_smem(k_spmv_q2<float, double>, s2d);
-        set_smem(k_spmv_q2<double, double>, s2d);
+        set_level_smem<float, float>();
+        set_level_smem<float, double>();
+        set_level_smem<double, double>();
+        g_ctas_per_sm[0] = level_occupancy<float, float>();
+        g_ctas_per_sm[1] = level_occupancy<float, double>();
+        g_ctas_per_sm[2] = level_occupancy<double, double>();
     });
 }
 
@@ -287,9 +300,14 @@ Problem* create_problem(const gb_lp* lp, const gb_options* opt) {
     P->red_partials.reset(kRedGrid);
 
     // schedules (host, from the row-length histogram) and transpose
-    P->A.sched.upload(build_schedule(P->A.host_ptr.data(), m), 3, s);
+        const int pgrid[kPartitions] = {P->sms * g_ctas_per_sm[0], P->sms * g_ctas_per_sm[1], P->sms * g_ctas_per_sm[2]};
+    P->st.reset(1);
+    GB_CUDA(cudaMemsetAsync(P->st.get(), 0, sizeof(SolveState), s));
+    unsigned* errp = &P->st.get()->err;
+    P->A.err = P->AT.err = P->Q.err = errp;
+    P->A.sched.upload(build_schedule(P->A.host_ptr.data(), m), 3, s, pgrid);
     device_transpose(*P, s);
-    P->AT.sched.upload(build_schedule(P->AT.host_ptr.data(), n), 3, s);
+    P->AT.sched.upload(build_schedule(P->AT.host_ptr.data(), n), 3, s, pgrid);
 
     // Ruiz equilibration + Pock-Chambolle (scaling.cpp:47-72)
     const int gw = elem_grid(static_cast<long long>(std::max(m, n)) * 32, P->sms);
@@ -335,7 +353,7 @@ Problem* create_problem(const gb_lp* lp, const gb_options* opt) {
     P->v64.alloc(n, m, P->qk, P->has_q);
     if (P->has_q && !P->dplr) {
         upload_mat(P->Q, n, n, lp->q_ptr, lp->q_idx, lp->q_val, s);
-        P->Q.sched.upload(build_schedule(P->Q.host_ptr.data(), n), 3, s);
+        P->Q.sched.upload(build_schedule(P->Q.host_ptr.data(), n), 3, s, pgrid);
         P->q_row_of.reset(P->Q.nnz ? P->Q.nnz : 1);
         k_row_of<<<elem_grid((long long)n * 32, P->sms), kThreads, 0, s>>>(n, P->Q.ptr.get(), P->q_row_of.get());
         k_scale_q<<<elem_grid(P->Q.nnz, P->sms), kThreads, 0, s>>>(static_cast<int>(P->Q.nnz), P->q_row_of.get(),
@@ -357,7 +375,8 @@ Problem* create_problem(const gb_lp* lp, const gb_options* opt) {
     k_w0<<<1, 1, 0, s>>>(sc, sc + 10, sc + 11);
     // FP32 copies of the matrix values and data
     auto cvt32 = [&](DevMat& M) {
-        M.val32.reset(M.nnz ? M.nnz : 1);
+        M.val32.reset(padded_nnz(M.nnz));
+        GB_CUDA(cudaMemsetAsync(M.val32.get(), 0, M.val32.size() * sizeof(float), s));
         if (M.nnz) k_convert<float><<<elem_grid(M.nnz, P->sms), kThreads, 0, s>>>(M.nnz, M.val64.get(), M.val32.get());
     };
     cvt32(P->A);
@@ -365,10 +384,11 @@ Problem* create_problem(const gb_lp* lp, const gb_options* opt) {
     if (P->has_q && !P->dplr) cvt32(P->Q);
     convert_data(*P, P->v32, s);
     convert_data(*P, P->v64, s);
-    P->st.reset(1);
     GB_CUDA(cudaMallocHost(&P->st_host, sizeof(SolveState)));
     GB_CUDA(cudaMemcpyAsync(P->scal_host, sc, 10 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaMemcpyAsync(P->st_host, P->st.get(), sizeof(SolveState), cudaMemcpyDeviceToHost, s));
     GB_CUDA(cudaStreamSynchronize(s));
+    if (P->st_host->err) throw Error(GB_ERR_CUDA, "a bounded wait for a TMA bulk copy gave up during setup");
     GB_CUDA(cudaGetLastError());
     P->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return P.release();
@@ -401,7 +421,8 @@ void launch_qx(Problem& P, VecSet<V>& vs, const V* x, V* qx, cudaStream_t s, lon
             P.n, P.qk, vs.F.get(), vs.D.get(), t, x, nullptr, nullptr, qx, nullptr);
         nl += 3;
     } else {
-        k_spmv<M, V><<<P.Q.sched.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(P.Q.view<M>(), x, qx);
+        constexpr int part = level_index<M, V>();
+        k_spmv<M, V><<<P.Q.sched.ctas(part), kThreads, spmv_smem_bytes_tma<1, M, V>(), s>>>(P.Q.view<M>(part), x, qx);
         nl += 1;
     }
 }
@@ -417,7 +438,8 @@ void launch_qx2(Problem& P, VecSet<V>& vs, const V* x, cudaStream_t s, long long
             P.n, P.qk, vs.F.get(), vs.D.get(), t, x, vs.sumx.get(), P.st.get(), vs.qx.get(), vs.qxa.get());
         nl += 3;
     } else {
-        k_spmv_q2<M, V><<<P.Q.sched.nb, kThreads, spmv_smem_bytes<2, V>(), s>>>(P.Q.view<M>(), x, vs.sumx.get(),
+        constexpr int part = level_index<M, V>();
+        k_spmv_q2<M, V><<<P.Q.sched.ctas(part), kThreads, spmv_smem_bytes_tma<2, M, V>(), s>>>(P.Q.view<M>(part), x, vs.sumx.get(),
                                                                             P.st.get(), vs.qx.get(), vs.qxa.get());
         nl += 1;
     }
@@ -426,8 +448,8 @@ void launch_qx2(Problem& P, VecSet<V>& vs, const V* x, cudaStream_t s, long long
 template <class M, class V>
 EvalArgs<M, V> eval_args(Problem& P, VecSet<V>& vs, const V* x, const V* y, int mode, bool with_q) {
     EvalArgs<M, V> a;
-    a.A = P.A.view<M>();
-    a.AT = P.AT.view<M>();
+    a.A = P.A.view<M>(level_index<M, V>());
+    a.AT = P.AT.view<M>(level_index<M, V>());
     a.x = x;
     a.y = y;
     a.sumx = vs.sumx.get();
@@ -459,17 +481,21 @@ void launch_iteration(Problem& P, VecSet<V>& vs, int k, cudaStream_t s, long lon
     const V* yin = (k & 1) ? vs.y1.get() : vs.y0.get();
     V* yout = (k & 1) ? vs.y0.get() : vs.y1.get();
     if (P.has_q) launch_qx<M, V>(P, vs, xin, vs.qx.get(), s, nl);
-    PrimalArgs<M, V> pa{P.AT.view<M>(), yin, xin, vs.c.get(), vs.l.get(), vs.u.get(),
+    constexpr int part = level_index<M, V>();
+    constexpr size_t sm = spmv_smem_bytes_tma<1, M, V>();
+    PrimalArgs<M, V> pa{P.AT.view<M>(part), yin, xin, vs.c.get(), vs.l.get(), vs.u.get(),
                         P.has_q ? vs.qx.get() : nullptr, xout, vs.xbar.get(), vs.sumx.get(), P.st.get()};
-    k_primal<M, V><<<P.AT.sched.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(pa);
-    DualArgs<M, V> da{P.A.view<M>(), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(), P.st.get()};
-    k_dual<M, V><<<P.A.sched.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(da);
+    k_primal<M, V><<<P.AT.sched.ctas(part), kThreads, sm, s>>>(pa);
+    DualArgs<M, V> da{P.A.view<M>(part), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(),
+                      P.st.get()};
+    k_dual<M, V><<<P.A.sched.ctas(part), kThreads, sm, s>>>(da);
     nl += 2;
 }
 
 // Body of the phase loop: check_every iterations, KKT check, restart.
+// use_cond = 0 when the body is launched from the host loop instead of the graph.
 template <class M, class V>
-long long capture_body(Problem& P, int ce, cudaGraphConditionalHandle cond, cudaStream_t s) {
+long long capture_body(Problem& P, int ce, cudaGraphConditionalHandle cond, cudaStream_t s, int use_cond = 1) {
     VecSet<V>& vs = Level<M, V>::vs(P);
     long long nl = 0;
     for (int k = 0; k < ce; ++k) launch_iteration<M, V>(P, vs, k, s, nl);
@@ -479,9 +505,10 @@ long long capture_body(Problem& P, int ce, cudaGraphConditionalHandle cond, cuda
     if (P.has_q) launch_qx2<M, V>(P, vs, xc, s, nl);
     EvalArgs<M, V> ea = eval_args<M, V>(P, vs, xc, yc, kEvalCheck, P.has_q);
     ea.cond = cond;
-    ea.use_cond = 1;
-    const int grid = P.A.sched.nb + P.AT.sched.nb;
-    k_eval<M, V, 2, 3><<<grid, kThreads, spmv_smem_bytes<3, V>(), s>>>(ea);
+    ea.use_cond = use_cond;
+    constexpr int part = level_index<M, V>();
+    const int grid = P.A.sched.ctas(part) + P.AT.sched.ctas(part);
+    k_eval<M, V, 2, 3><<<grid, kThreads, spmv_smem_bytes_tma<3, M, V>(), s>>>(ea);
     RestartArgs<V> ra{xc, yc, vs.x0.get(), vs.y0.get(), vs.xr.get(), vs.yr.get(), vs.sumx.get(), vs.sumy.get(),
                       P.n, P.m, P.st.get()};
     k_restart<V><<<elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s>>>(ra);
@@ -527,6 +554,17 @@ LevelGraph* level_graph(Problem& P, int ce) {
     return g;
 }
 
+// GANIT_B200_LAUNCH=stream runs each phase loop from the host (same kernels,
+// one state read-back per check) instead of the device-side while loop of a
+// conditional CUDA graph; kernel profilers need it to see the loop's kernels.
+bool host_loop_mode() {
+    static const bool host = [] {
+        const char* v = std::getenv("GANIT_B200_LAUNCH");
+        return v != nullptr && std::string(v) == "stream";
+    }();
+    return host;
+}
+
 __global__ void k_set_phase(SolveState* st, double tol, int stall_checks, int stall_exit, int first_phase) {
     st->phase_tol = tol;
     st->stall_checks = stall_checks;
@@ -559,6 +597,8 @@ __global__ void k_init_state(SolveState* st, const double* sc, double obj_const,
 void sync_state(Problem& P) {
     GB_CUDA(cudaMemcpyAsync(P.st_host, P.st.get(), sizeof(SolveState), cudaMemcpyDeviceToHost, P.stream));
     GB_CUDA(cudaStreamSynchronize(P.stream));
+    if (P.st_host->err)
+        throw Error(GB_ERR_CUDA, "a bounded wait for a TMA bulk copy gave up (results of this solve are invalid)");
 }
 
 template <class M, class V>
@@ -574,16 +614,29 @@ int run_phase(Problem& P, const gb_options* opt, double tol, int stall_exit, int
     P.launches += 2;
     if (P.has_q) launch_qx<M, V>(P, vs, vs.x0.get(), vs.qx.get(), s, P.launches);
     EvalArgs<M, V> ea = eval_args<M, V>(P, vs, vs.x0.get(), vs.y0.get(), kEvalInit, P.has_q);
-    k_eval<M, V, 1, 1><<<P.A.sched.nb + P.AT.sched.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(ea);
+    constexpr int part = level_index<M, V>();
+    k_eval<M, V, 1, 1><<<P.A.sched.ctas(part) + P.AT.sched.ctas(part), kThreads, spmv_smem_bytes_tma<1, M, V>(), s>>>(ea);
     P.launches += 1;
-    LevelGraph* g = level_graph<M, V>(P, opt->check_every);
     const int checks_before = first ? 0 : P.st_host->checks;
-    GB_CUDA(cudaGraphLaunch(g->exec, s));
+    long long per_body = 0;
+    if (host_loop_mode()) {
+        // Same kernels, launched from a host loop with one state read-back per
+        // check (profilers cannot see kernels inside conditional graphs).
+        for (;;) {
+            per_body = capture_body<M, V>(P, opt->check_every, 0, s, 0);
+            sync_state(P);
+            if (P.st_host->done) break;
+        }
+    } else {
+        LevelGraph* g = level_graph<M, V>(P, opt->check_every);
+        GB_CUDA(cudaGraphLaunch(g->exec, s));
+        per_body = g->launches_per_body;
+    }
     k_phase_out<V><<<gv, kThreads, 0, s>>>(P.n, P.m, vs.x0.get(), vs.y0.get(), vs.sumx.get(), vs.sumy.get(),
                                           vs.xr.get(), vs.yr.get(), P.st.get(), P.x64.get(), P.y64.get(),
                                           P.xr64.get(), P.yr64.get());
     sync_state(P);
-    P.launches += 1 + static_cast<long long>(P.st_host->checks - checks_before) * g->launches_per_body;
+    P.launches += 1 + static_cast<long long>(P.st_host->checks - checks_before) * per_body;
     GB_CUDA(cudaGetLastError());
     return P.st_host->exit_reason;
 }
@@ -594,7 +647,8 @@ Kkt certify(Problem& P) {
     VecSet<double>& vs = P.v64;
     if (P.has_q) launch_qx<double, double>(P, vs, P.x64.get(), vs.qx.get(), s, P.launches);
     EvalArgs<double, double> ea = eval_args<double, double>(P, vs, P.x64.get(), P.y64.get(), kEvalCertify, P.has_q);
-    k_eval<double, double, 1, 1><<<P.A.sched.nb + P.AT.sched.nb, kThreads, spmv_smem_bytes<1, double>(), s>>>(ea);
+    k_eval<double, double, 1, 1><<<P.A.sched.ctas(2) + P.AT.sched.ctas(2), kThreads,
+                                   spmv_smem_bytes_tma<1, double, double>(), s>>>(ea);
     P.launches += 1;
     sync_state(P);
     return P.st_host->kcert;
@@ -707,13 +761,15 @@ void time_level(Problem& P, int iters, double* msp, double* msd, int64_t* launch
         const V* yin = (k & 1) ? vs.y1.get() : vs.y0.get();
         V* yout = (k & 1) ? vs.y0.get() : vs.y1.get();
         if (P.has_q) launch_qx<M, V>(P, vs, xin, vs.qx.get(), s, nl);
-        PrimalArgs<M, V> pa{P.AT.view<M>(), yin, xin, vs.c.get(), vs.l.get(), vs.u.get(),
+        constexpr int part = level_index<M, V>();
+        constexpr size_t sm = spmv_smem_bytes_tma<1, M, V>();
+        PrimalArgs<M, V> pa{P.AT.view<M>(part), yin, xin, vs.c.get(), vs.l.get(), vs.u.get(),
                             P.has_q ? vs.qx.get() : nullptr, xout, vs.xbar.get(), vs.sumx.get(), P.st.get()};
-        k_primal<M, V><<<P.AT.sched.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(pa);
+        k_primal<M, V><<<P.AT.sched.ctas(part), kThreads, sm, s>>>(pa);
         GB_CUDA(cudaEventRecord(ev[2 * k + 1], s));
-        DualArgs<M, V> da{P.A.view<M>(), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(),
+        DualArgs<M, V> da{P.A.view<M>(part), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(),
                           P.st.get()};
-        k_dual<M, V><<<P.A.sched.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(da);
+        k_dual<M, V><<<P.A.sched.ctas(part), kThreads, sm, s>>>(da);
         GB_CUDA(cudaEventRecord(ev[2 * k + 2], s));
         nl += 2;
     }

@@ -52,6 +52,7 @@ struct alignas(16) SolveState {
     double inv_avg;
     Kkt best, kcert, kc, ka;
     unsigned arrive;           // CTA arrival counter of k_eval (re-armed by the last CTA)
+    unsigned err;              // set by a bounded wait that gave up
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -76,29 +77,40 @@ struct PrimalArgs {
     const SolveState* st;
 };
 
-template <class M, class V>
+template <class V>
 struct PrimalEpi {
-    const PrimalArgs<M, V>& a;
+    const V* __restrict__ x;
+    const V* __restrict__ c;
+    const V* __restrict__ l;
+    const V* __restrict__ u;
+    const V* __restrict__ qx;
+    V* __restrict__ xn;
+    V* __restrict__ xbar;
+    V* __restrict__ sumx;
     V tau;
-    __device__ __forceinline__ void operator()(int j, const V (&s)[1]) {
-        const V xj = a.x[j];
-        const V g = a.c[j] - s[0] + (a.qx ? a.qx[j] : V(0));
-        V v = xj - tau * g;
-        const V lj = a.l[j], uj = a.u[j];
-        v = (v < lj) ? lj : v;
-        v = (uj < v) ? uj : v;
-        a.xn[j] = v;
-        a.xbar[j] = V(2) * v - xj;
-        a.sumx[j] += v;
+    struct Pre {
+        V x, c, l, u, sumx, qx;
+    };
+    __device__ __forceinline__ Pre prefetch(int j) const {
+        return Pre{x[j], c[j], l[j], u[j], sumx[j], qx ? qx[j] : V(0)};
+    }
+    __device__ __forceinline__ void operator()(int j, const V (&s)[1], const Pre& p) {
+        const V g = p.c - s[0] + p.qx;
+        V v = p.x - tau * g;
+        v = (v < p.l) ? p.l : v;
+        v = (p.u < v) ? p.u : v;
+        xn[j] = v;
+        xbar[j] = V(2) * v - p.x;
+        sumx[j] = p.sumx + v;
     }
 };
 
 template <class M, class V>
-__global__ void __launch_bounds__(kThreads) k_primal(const PrimalArgs<M, V> a) {
+__global__ void __launch_bounds__(kThreads, sizeof(V) == 4 ? 4 : 2) k_primal(const PrimalArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const RowBlock b = a.AT.blocks[blockIdx.x];
-    PrimalEpi<M, V> epi{a, static_cast<V>(a.st->tau)};
-    spmv_block<1, M, V>(a.AT, b, GatherOne<V>{a.y}, epi, smem);
+    PrimalEpi<V> epi{a.x, a.c, a.l, a.u, a.qx, a.xn, a.xbar, a.sumx, static_cast<V>(a.st->tau)};
+    const CsrView<M> AT = a.AT;
+    spmv_run<1, M, V>(AT, blockIdx.x, GatherOne<V>{a.y}, epi, smem);
 }
 
 template <class M, class V>
@@ -113,28 +125,36 @@ struct DualArgs {
     const SolveState* st;
 };
 
-template <class M, class V>
+template <class V>
 struct DualEpi {
-    const DualArgs<M, V>& a;
+    const V* __restrict__ y;
+    const V* __restrict__ lo;
+    const V* __restrict__ hi;
+    V* __restrict__ yn;
+    V* __restrict__ sumy;
     V sigma;
-    __device__ __forceinline__ void operator()(int i, const V (&s)[1]) {
-        const V q = a.y[i] - sigma * s[0];
-        const V lo = sigma * a.lo[i], hi = sigma * a.hi[i];
+    struct Pre {
+        V y, lo, hi, sumy;
+    };
+    __device__ __forceinline__ Pre prefetch(int i) const { return Pre{y[i], lo[i], hi[i], sumy[i]}; }
+    __device__ __forceinline__ void operator()(int i, const V (&s)[1], const Pre& p) {
+        const V q = p.y - sigma * s[0];
+        const V l = sigma * p.lo, h = sigma * p.hi;
         V t = -q;
-        t = (t < lo) ? lo : t;
-        t = (hi < t) ? hi : t;
+        t = (t < l) ? l : t;
+        t = (h < t) ? h : t;
         const V v = q + t;
-        a.yn[i] = v;
-        a.sumy[i] += v;
+        yn[i] = v;
+        sumy[i] = p.sumy + v;
     }
 };
 
 template <class M, class V>
-__global__ void __launch_bounds__(kThreads) k_dual(const DualArgs<M, V> a) {
+__global__ void __launch_bounds__(kThreads, sizeof(V) == 4 ? 4 : 2) k_dual(const DualArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const RowBlock b = a.A.blocks[blockIdx.x];
-    DualEpi<M, V> epi{a, static_cast<V>(a.st->sigma)};
-    spmv_block<1, M, V>(a.A, b, GatherOne<V>{a.xbar}, epi, smem);
+    DualEpi<V> epi{a.y, a.lo, a.hi, a.yn, a.sumy, static_cast<V>(a.st->sigma)};
+    const CsrView<M> A = a.A;
+    spmv_run<1, M, V>(A, blockIdx.x, GatherOne<V>{a.xbar}, epi, smem);
 }
 
 // ---------------------------------------------------------------- KKT evaluation
@@ -205,7 +225,7 @@ struct GatherYAvgRay {  // A^T side: y, ya and the ray y - yr
 // Per-row terms (backend_cpu.cpp:101-112, 132-142) and restart distances.
 template <class M, class V, int NV>
 struct EvalRowEpi {
-    const EvalArgs<M, V>& a;
+    EvalArgs<M, V> a;
     double inv;
     double t[kTerms];
     __device__ __forceinline__ static double pres2(double ax, double lo, double hi, double r) {
@@ -219,7 +239,8 @@ struct EvalRowEpi {
         if (yi < 0 && isfinite(hi)) return yi * hi;
         return 0.0;
     }
-    __device__ __forceinline__ void operator()(int i, const V (&s)[NV]) {
+    __device__ __forceinline__ NoPre prefetch(int) const { return {}; }
+    __device__ __forceinline__ void operator()(int i, const V (&s)[NV], const NoPre&) {
         const double lo = double(a.lo[i]), hi = double(a.hi[i]), r = double(a.rres[i]);
         const V yi = a.y[i];
         t[T_RP2_C] += pres2(double(s[0]), lo, hi, r);
@@ -241,7 +262,7 @@ struct EvalRowEpi {
 // Per-column terms (backend_cpu.cpp:113-131, 143-149).
 template <class M, class V, int NV>
 struct EvalColEpi {
-    const EvalArgs<M, V>& a;
+    EvalArgs<M, V> a;
     double inv;
     double t[kTerms];
     __device__ __forceinline__ static void dres(double z, double lj, double uj, double cres, double& rd2,
@@ -252,7 +273,8 @@ struct EvalColEpi {
         r /= cres;
         rd2 += r * r;
     }
-    __device__ __forceinline__ void operator()(int j, const V (&s)[NV]) {
+    __device__ __forceinline__ NoPre prefetch(int) const { return {}; }
+    __device__ __forceinline__ void operator()(int j, const V (&s)[NV], const NoPre&) {
         const double cj = double(a.c[j]), lj = double(a.l[j]), uj = double(a.u[j]), cr = double(a.cres[j]);
         const V xj = a.x[j];
         const double qc = a.qx ? double(a.qx[j]) : 0.0;
@@ -386,25 +408,25 @@ __global__ void __launch_bounds__(kThreads) k_eval(const EvalArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double red[kWarps * kTerms];
     __shared__ bool am_last;
-    const int nbA = a.A.nb;
+    const int nctaA = a.A.ncta;
     const double inv = (a.mode == kEvalCheck)
                            ? 1.0 / static_cast<double>(a.st->it_since + a.st->check_every)
                            : 0.0;
     double t[kTerms];
-    if (static_cast<int>(blockIdx.x) < nbA) {
-        const RowBlock b = a.A.blocks[blockIdx.x];
+    if (static_cast<int>(blockIdx.x) < nctaA) {
         EvalRowEpi<M, V, NVA> epi{a, inv, {}};
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) epi.t[k] = 0.0;
-        spmv_block<NVA, M, V>(a.A, b, GatherXAvg<V, NVA>{a.x, a.sumx, inv}, epi, smem);
+        const CsrView<M> A = a.A;
+        spmv_run<NVA, M, V>(A, blockIdx.x, GatherXAvg<V, NVA>{a.x, a.sumx, inv}, epi, smem);
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) t[k] = epi.t[k];
     } else {
-        const RowBlock b = a.AT.blocks[blockIdx.x - nbA];
         EvalColEpi<M, V, NVT> epi{a, inv, {}};
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) epi.t[k] = 0.0;
-        spmv_block<NVT, M, V>(a.AT, b, GatherYAvgRay<V, NVT>{a.y, a.sumy, a.yr, inv}, epi, smem);
+        const CsrView<M> AT = a.AT;
+        spmv_run<NVT, M, V>(AT, blockIdx.x - nctaA, GatherYAvgRay<V, NVT>{a.y, a.sumy, a.yr, inv}, epi, smem);
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) t[k] = epi.t[k];
     }

@@ -17,7 +17,8 @@ template <class V>
 struct Store2Epi {
     V* __restrict__ y0;
     V* __restrict__ y1;
-    __device__ __forceinline__ void operator()(int r, const V (&s)[2]) {
+    __device__ __forceinline__ NoPre prefetch(int) const { return {}; }
+    __device__ __forceinline__ void operator()(int r, const V (&s)[2], const NoPre&) {
         y0[r] = s[0];
         y1[r] = s[1];
     }
@@ -29,9 +30,9 @@ __global__ void __launch_bounds__(kThreads) k_spmv_q2(const CsrView<M> Q, const 
                                                      V* __restrict__ qx, V* __restrict__ qxa) {
     extern __shared__ __align__(16) unsigned char smem[];
     const double inv = 1.0 / static_cast<double>(st->it_since + st->check_every);
-    const RowBlock b = Q.blocks[blockIdx.x];
     Store2Epi<V> epi{qx, qxa};
-    spmv_block<2, M, V>(Q, b, GatherXAvg<V, 2>{x, sumx, inv}, epi, smem);
+    const CsrView<M> Qv = Q;
+    spmv_run<2, M, V>(Qv, blockIdx.x, GatherXAvg<V, 2>{x, sumx, inv}, epi, smem);
 }
 
 // Partial F^T v for NV vectors: v0 = x, v1 = inv * sumx (when NV == 2).

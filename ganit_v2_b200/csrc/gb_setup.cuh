@@ -69,14 +69,16 @@ inline void reduce_to(cudaStream_t s, long long n, F f, double* partials, double
 template <class V>
 struct StoreEpi {
     V* __restrict__ y;
-    __device__ __forceinline__ void operator()(int r, const V (&s)[1]) { y[r] = s[0]; }
+    __device__ __forceinline__ NoPre prefetch(int) const { return {}; }
+    __device__ __forceinline__ void operator()(int r, const V (&s)[1], const NoPre&) { y[r] = s[0]; }
 };
 template <class M, class V>
-__global__ void __launch_bounds__(kThreads) k_spmv(const CsrView<M> A, const V* __restrict__ x, V* __restrict__ y) {
+__global__ void __launch_bounds__(kThreads, sizeof(V) == 4 ? 4 : 2) k_spmv(const CsrView<M> A, const V* __restrict__ x,
+                                                     V* __restrict__ y) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const RowBlock b = A.blocks[blockIdx.x];
     StoreEpi<V> epi{y};
-    spmv_block<1, M, V>(A, b, GatherOne<V>{x}, epi, smem);
+    const CsrView<M> Av = A;
+    spmv_run<1, M, V>(Av, blockIdx.x, GatherOne<V>{x}, epi, smem);
 }
 
 // ---------------------------------------------------------------- transpose / scaling kernels
