@@ -200,9 +200,6 @@ CsrView<M> bview(const DevBuf<int>& ptr, const DevBuf<int>& idx, const DevBuf<un
     v.idx = idx.get();
     v.val = reinterpret_cast<const M*>(val.get());
     v.blocks = s.blocks.get();
-    v.cta_start = nullptr;
-    v.ncta = s.nb;
-    v.err = nullptr;
     v.slots = s.slots.get();
     v.counters = s.counters.get();
     v.rows = rows;

@@ -100,50 +100,6 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
-// ---- TMA bulk copies (non-tensor) and mbarriers, sm_90+ PTX.
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-// Orders this thread's generic-proxy shared-memory accesses before later
-// async-proxy (TMA) writes to the same buffer.
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
-    asm volatile(
-        "{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
-        "r"(bytes)
-        : "memory");
-}
-// Bulk global -> shared copy completing on `bar`; both addresses 16-byte
-// aligned, bytes a multiple of 16.  No multicast.
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait for the phase of `bar` with the given parity: gives up after
-// kMbarPollLimit polls (each try_wait may itself suspend briefly) and
-// returns false, so a lost copy can never hang the GPU.
-constexpr long long kMbarPollLimit = 1LL << 22;
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-    for (long long i = 0; i < kMbarPollLimit; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-
 // Deterministic block sum of K doubles held by every thread.  Result valid in
 // thread 0.  `sh` must hold kWarps*K doubles.  Order: shuffle tree inside each
 // warp, then warps 0..7 sequentially.

@@ -164,10 +164,10 @@ void power_norm_A(Problem& P, cudaStream_t s) {
     reduce_to(s, n, Sq{v}, P.red_partials.get(), pw, PostSqrt{});
     k_power_step<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, v, v, pw);  // v /= ||v|| (lambda overwritten below)
     GB_CUDA(cudaMemsetAsync(pw + 1, 0, 2 * sizeof(double), s));
-    const size_t sm1 = spmv_smem_bytes_tma<1, double, double>();
+    const size_t sm1 = spmv_smem_bytes<1, double>();
     for (int it = 0; it < 50; ++it) {
-        k_spmv<double, double><<<P.A.sched.ctas(2), kThreads, sm1, s>>>(P.A.view<double>(2), v, w);
-        k_spmv<double, double><<<P.AT.sched.ctas(2), kThreads, sm1, s>>>(P.AT.view<double>(2), w, z);
+        k_spmv<double, double><<<P.A.sched.nb, kThreads, sm1, s>>>(P.A.view<double>(), v, w);
+        k_spmv<double, double><<<P.AT.sched.nb, kThreads, sm1, s>>>(P.AT.view<double>(), w, z);
         reduce_to(s, n, Sq{z}, P.red_partials.get(), pw, PostSqrt{});
         k_power_step<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, z, v, pw);
     }
@@ -186,12 +186,12 @@ void power_norm_Q(Problem& P, cudaStream_t s) {
     reduce_to(s, n, Sq{v}, P.red_partials.get(), pw, PostSqrt{});
     k_power_step<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, v, v, pw);
     GB_CUDA(cudaMemsetAsync(pw + 1, 0, 2 * sizeof(double), s));
-    const size_t sm1 = spmv_smem_bytes_tma<1, double, double>();
+    const size_t sm1 = spmv_smem_bytes<1, double>();
     for (int it = 0; it < 60; ++it) {
         if (P.dplr)
             qx_dplr_f64(P, v, w, s);
         else
-            k_spmv<double, double><<<P.Q.sched.ctas(2), kThreads, sm1, s>>>(P.Q.view<double>(2), v, w);
+            k_spmv<double, double><<<P.Q.sched.nb, kThreads, sm1, s>>>(P.Q.view<double>(), v, w);
         reduce_to(s, n, Sq{w}, P.red_partials.get(), pw, PostSqrt{});
         k_power_step<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, w, v, pw);
     }
@@ -227,38 +227,15 @@ void convert_data(Problem& P, VecSet<V>& vs, cudaStream_t s) {
     }
 }
 
-// Resident CTAs per SM of the fused iteration kernels of each precision level
-// (L1 <f,f>, L2 <f,d>, L3 <d,d>): the persistent grids are one full wave.
-int g_ctas_per_sm[kPartitions] = {4, 4, 2};
-
-template <class M, class V>
-int level_occupancy() {
-    const size_t sm = spmv_smem_bytes_tma<1, M, V>();
-    int o1 = 0, o2 = 0;
-    GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_dual<M, V>, kThreads, sm));
-    GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_primal<M, V>, kThreads, sm));
-    return std::max(1, std::min(o1, o2));
-}
-
-template <class M, class V>
-void set_level_smem() {
-    set_smem(k_spmv<M, V>, spmv_smem_bytes_tma<1, M, V>());
-    set_smem(k_primal<M, V>, spmv_smem_bytes_tma<1, M, V>());
-    set_smem(k_dual<M, V>, spmv_smem_bytes_tma<1, M, V>());
-    set_smem(k_eval<M, V, 2, 3>, spmv_smem_bytes_tma<3, M, V>());
-    set_smem(k_eval<M, V, 1, 1>, spmv_smem_bytes_tma<1, M, V>());
-    set_smem(k_spmv_q2<M, V>, spmv_smem_bytes_tma<2, M, V>());
-}
-
+// Kernels whose dynamic shared memory exceeds the 48 KB default opt in.
 void init_kernel_attrs() {
     static std::once_flag once;
     std::call_once(once, [] {
-        set_level_smem<float, float>();
-        set_level_smem<float, double>();
-        set_level_smem<double, double>();
-        g_ctas_per_sm[0] = level_occupancy<float, float>();
-        g_ctas_per_sm[1] = level_occupancy<float, double>();
-        g_ctas_per_sm[2] = level_occupancy<double, double>();
+        set_smem(k_eval<float, float, 2, 3>, spmv_smem_bytes<3, float>());
+        set_smem(k_eval<float, double, 2, 3>, spmv_smem_bytes<3, double>());
+        set_smem(k_eval<double, double, 2, 3>, spmv_smem_bytes<3, double>());
+        set_smem(k_spmv_q2<float, double>, spmv_smem_bytes<2, double>());
+        set_smem(k_spmv_q2<double, double>, spmv_smem_bytes<2, double>());
     });
 }
 
@@ -300,14 +277,11 @@ Problem* create_problem(const gb_lp* lp, const gb_options* opt) {
     P->red_partials.reset(kRedGrid);
 
     // schedules (host, from the row-length histogram) and transpose
-        const int pgrid[kPartitions] = {P->sms * g_ctas_per_sm[0], P->sms * g_ctas_per_sm[1], P->sms * g_ctas_per_sm[2]};
-    P->st.reset(1);
+        P->st.reset(1);
     GB_CUDA(cudaMemsetAsync(P->st.get(), 0, sizeof(SolveState), s));
-    unsigned* errp = &P->st.get()->err;
-    P->A.err = P->AT.err = P->Q.err = errp;
-    P->A.sched.upload(build_schedule(P->A.host_ptr.data(), m), 3, s, pgrid);
+    P->A.sched.upload(build_schedule(P->A.host_ptr.data(), m), 3, s);
     device_transpose(*P, s);
-    P->AT.sched.upload(build_schedule(P->AT.host_ptr.data(), n), 3, s, pgrid);
+    P->AT.sched.upload(build_schedule(P->AT.host_ptr.data(), n), 3, s);
 
     // Ruiz equilibration + Pock-Chambolle (scaling.cpp:47-72)
     const int gw = elem_grid(static_cast<long long>(std::max(m, n)) * 32, P->sms);
@@ -353,7 +327,7 @@ Problem* create_problem(const gb_lp* lp, const gb_options* opt) {
     P->v64.alloc(n, m, P->qk, P->has_q);
     if (P->has_q && !P->dplr) {
         upload_mat(P->Q, n, n, lp->q_ptr, lp->q_idx, lp->q_val, s);
-        P->Q.sched.upload(build_schedule(P->Q.host_ptr.data(), n), 3, s, pgrid);
+        P->Q.sched.upload(build_schedule(P->Q.host_ptr.data(), n), 3, s);
         P->q_row_of.reset(P->Q.nnz ? P->Q.nnz : 1);
         k_row_of<<<elem_grid((long long)n * 32, P->sms), kThreads, 0, s>>>(n, P->Q.ptr.get(), P->q_row_of.get());
         k_scale_q<<<elem_grid(P->Q.nnz, P->sms), kThreads, 0, s>>>(static_cast<int>(P->Q.nnz), P->q_row_of.get(),
@@ -386,9 +360,7 @@ Problem* create_problem(const gb_lp* lp, const gb_options* opt) {
     convert_data(*P, P->v64, s);
     GB_CUDA(cudaMallocHost(&P->st_host, sizeof(SolveState)));
     GB_CUDA(cudaMemcpyAsync(P->scal_host, sc, 10 * sizeof(double), cudaMemcpyDeviceToHost, s));
-    GB_CUDA(cudaMemcpyAsync(P->st_host, P->st.get(), sizeof(SolveState), cudaMemcpyDeviceToHost, s));
     GB_CUDA(cudaStreamSynchronize(s));
-    if (P->st_host->err) throw Error(GB_ERR_CUDA, "a bounded wait for a TMA bulk copy gave up during setup");
     GB_CUDA(cudaGetLastError());
     P->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return P.release();
@@ -421,8 +393,7 @@ void launch_qx(Problem& P, VecSet<V>& vs, const V* x, V* qx, cudaStream_t s, lon
             P.n, P.qk, vs.F.get(), vs.D.get(), t, x, nullptr, nullptr, qx, nullptr);
         nl += 3;
     } else {
-        constexpr int part = level_index<M, V>();
-        k_spmv<M, V><<<P.Q.sched.ctas(part), kThreads, spmv_smem_bytes_tma<1, M, V>(), s>>>(P.Q.view<M>(part), x, qx);
+        k_spmv<M, V><<<P.Q.sched.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(P.Q.view<M>(), x, qx);
         nl += 1;
     }
 }
@@ -438,8 +409,7 @@ void launch_qx2(Problem& P, VecSet<V>& vs, const V* x, cudaStream_t s, long long
             P.n, P.qk, vs.F.get(), vs.D.get(), t, x, vs.sumx.get(), P.st.get(), vs.qx.get(), vs.qxa.get());
         nl += 3;
     } else {
-        constexpr int part = level_index<M, V>();
-        k_spmv_q2<M, V><<<P.Q.sched.ctas(part), kThreads, spmv_smem_bytes_tma<2, M, V>(), s>>>(P.Q.view<M>(part), x, vs.sumx.get(),
+        k_spmv_q2<M, V><<<P.Q.sched.nb, kThreads, spmv_smem_bytes<2, V>(), s>>>(P.Q.view<M>(), x, vs.sumx.get(),
                                                                             P.st.get(), vs.qx.get(), vs.qxa.get());
         nl += 1;
     }
@@ -448,8 +418,8 @@ void launch_qx2(Problem& P, VecSet<V>& vs, const V* x, cudaStream_t s, long long
 template <class M, class V>
 EvalArgs<M, V> eval_args(Problem& P, VecSet<V>& vs, const V* x, const V* y, int mode, bool with_q) {
     EvalArgs<M, V> a;
-    a.A = P.A.view<M>(level_index<M, V>());
-    a.AT = P.AT.view<M>(level_index<M, V>());
+    a.A = P.A.view<M>();
+    a.AT = P.AT.view<M>();
     a.x = x;
     a.y = y;
     a.sumx = vs.sumx.get();
@@ -481,14 +451,13 @@ void launch_iteration(Problem& P, VecSet<V>& vs, int k, cudaStream_t s, long lon
     const V* yin = (k & 1) ? vs.y1.get() : vs.y0.get();
     V* yout = (k & 1) ? vs.y0.get() : vs.y1.get();
     if (P.has_q) launch_qx<M, V>(P, vs, xin, vs.qx.get(), s, nl);
-    constexpr int part = level_index<M, V>();
-    constexpr size_t sm = spmv_smem_bytes_tma<1, M, V>();
-    PrimalArgs<M, V> pa{P.AT.view<M>(part), yin, xin, vs.c.get(), vs.l.get(), vs.u.get(),
+    constexpr size_t sm = spmv_smem_bytes<1, V>();
+    PrimalArgs<M, V> pa{P.AT.view<M>(), yin, xin, vs.c.get(), vs.l.get(), vs.u.get(),
                         P.has_q ? vs.qx.get() : nullptr, xout, vs.xbar.get(), vs.sumx.get(), P.st.get()};
-    k_primal<M, V><<<P.AT.sched.ctas(part), kThreads, sm, s>>>(pa);
-    DualArgs<M, V> da{P.A.view<M>(part), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(),
+    k_primal<M, V><<<P.AT.sched.nb, kThreads, sm, s>>>(pa);
+    DualArgs<M, V> da{P.A.view<M>(), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(),
                       P.st.get()};
-    k_dual<M, V><<<P.A.sched.ctas(part), kThreads, sm, s>>>(da);
+    k_dual<M, V><<<P.A.sched.nb, kThreads, sm, s>>>(da);
     nl += 2;
 }
 
@@ -506,9 +475,8 @@ long long capture_body(Problem& P, int ce, cudaGraphConditionalHandle cond, cuda
     EvalArgs<M, V> ea = eval_args<M, V>(P, vs, xc, yc, kEvalCheck, P.has_q);
     ea.cond = cond;
     ea.use_cond = use_cond;
-    constexpr int part = level_index<M, V>();
-    const int grid = P.A.sched.ctas(part) + P.AT.sched.ctas(part);
-    k_eval<M, V, 2, 3><<<grid, kThreads, spmv_smem_bytes_tma<3, M, V>(), s>>>(ea);
+    const int grid = P.A.sched.nb + P.AT.sched.nb;
+    k_eval<M, V, 2, 3><<<grid, kThreads, spmv_smem_bytes<3, V>(), s>>>(ea);
     RestartArgs<V> ra{xc, yc, vs.x0.get(), vs.y0.get(), vs.xr.get(), vs.yr.get(), vs.sumx.get(), vs.sumy.get(),
                       P.n, P.m, P.st.get()};
     k_restart<V><<<elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s>>>(ra);
@@ -597,8 +565,6 @@ __global__ void k_init_state(SolveState* st, const double* sc, double obj_const,
 void sync_state(Problem& P) {
     GB_CUDA(cudaMemcpyAsync(P.st_host, P.st.get(), sizeof(SolveState), cudaMemcpyDeviceToHost, P.stream));
     GB_CUDA(cudaStreamSynchronize(P.stream));
-    if (P.st_host->err)
-        throw Error(GB_ERR_CUDA, "a bounded wait for a TMA bulk copy gave up (results of this solve are invalid)");
 }
 
 template <class M, class V>
@@ -614,8 +580,7 @@ int run_phase(Problem& P, const gb_options* opt, double tol, int stall_exit, int
     P.launches += 2;
     if (P.has_q) launch_qx<M, V>(P, vs, vs.x0.get(), vs.qx.get(), s, P.launches);
     EvalArgs<M, V> ea = eval_args<M, V>(P, vs, vs.x0.get(), vs.y0.get(), kEvalInit, P.has_q);
-    constexpr int part = level_index<M, V>();
-    k_eval<M, V, 1, 1><<<P.A.sched.ctas(part) + P.AT.sched.ctas(part), kThreads, spmv_smem_bytes_tma<1, M, V>(), s>>>(ea);
+    k_eval<M, V, 1, 1><<<P.A.sched.nb + P.AT.sched.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(ea);
     P.launches += 1;
     const int checks_before = first ? 0 : P.st_host->checks;
     long long per_body = 0;
@@ -647,8 +612,8 @@ Kkt certify(Problem& P) {
     VecSet<double>& vs = P.v64;
     if (P.has_q) launch_qx<double, double>(P, vs, P.x64.get(), vs.qx.get(), s, P.launches);
     EvalArgs<double, double> ea = eval_args<double, double>(P, vs, P.x64.get(), P.y64.get(), kEvalCertify, P.has_q);
-    k_eval<double, double, 1, 1><<<P.A.sched.ctas(2) + P.AT.sched.ctas(2), kThreads,
-                                   spmv_smem_bytes_tma<1, double, double>(), s>>>(ea);
+    k_eval<double, double, 1, 1><<<P.A.sched.nb + P.AT.sched.nb, kThreads,
+                                   spmv_smem_bytes<1, double>(), s>>>(ea);
     P.launches += 1;
     sync_state(P);
     return P.st_host->kcert;
@@ -761,15 +726,14 @@ void time_level(Problem& P, int iters, double* msp, double* msd, int64_t* launch
         const V* yin = (k & 1) ? vs.y1.get() : vs.y0.get();
         V* yout = (k & 1) ? vs.y0.get() : vs.y1.get();
         if (P.has_q) launch_qx<M, V>(P, vs, xin, vs.qx.get(), s, nl);
-        constexpr int part = level_index<M, V>();
-        constexpr size_t sm = spmv_smem_bytes_tma<1, M, V>();
-        PrimalArgs<M, V> pa{P.AT.view<M>(part), yin, xin, vs.c.get(), vs.l.get(), vs.u.get(),
+        constexpr size_t sm = spmv_smem_bytes<1, V>();
+        PrimalArgs<M, V> pa{P.AT.view<M>(), yin, xin, vs.c.get(), vs.l.get(), vs.u.get(),
                             P.has_q ? vs.qx.get() : nullptr, xout, vs.xbar.get(), vs.sumx.get(), P.st.get()};
-        k_primal<M, V><<<P.AT.sched.ctas(part), kThreads, sm, s>>>(pa);
+        k_primal<M, V><<<P.AT.sched.nb, kThreads, sm, s>>>(pa);
         GB_CUDA(cudaEventRecord(ev[2 * k + 1], s));
-        DualArgs<M, V> da{P.A.view<M>(part), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(),
+        DualArgs<M, V> da{P.A.view<M>(), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(),
                           P.st.get()};
-        k_dual<M, V><<<P.A.sched.ctas(part), kThreads, sm, s>>>(da);
+        k_dual<M, V><<<P.A.sched.nb, kThreads, sm, s>>>(da);
         GB_CUDA(cudaEventRecord(ev[2 * k + 2], s));
         nl += 2;
     }

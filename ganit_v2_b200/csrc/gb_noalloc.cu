@@ -116,11 +116,9 @@ extern "C" int gb_eval_kkt_noalloc(const gb_scaled_lp* dev, const int32_t* h_a_p
         std::memset(&a, 0, sizeof(a));
         a.A.ptr = dev->a_ptr; a.A.idx = dev->a_idx; a.A.val = dev->a_val;
         a.A.blocks = blocks; a.A.slots = slots; a.A.counters = counters; a.A.rows = dev->m; a.A.nb = nbA;
-        a.A.cta_start = nullptr; a.A.ncta = nbA;
         a.AT.ptr = dev->at_ptr; a.AT.idx = dev->at_idx; a.AT.val = dev->at_val;
         a.AT.blocks = blocks + nbA; a.AT.slots = slots + slotsA; a.AT.counters = counters + countersA;
         a.AT.rows = dev->n; a.AT.nb = nb - nbA;
-        a.AT.cta_start = nullptr; a.AT.ncta = nb - nbA;
         a.x = x; a.y = y;
         a.c = dev->c; a.l = dev->l; a.u = dev->u; a.lo = dev->lo; a.hi = dev->hi; a.rres = dev->rres; a.cres = dev->cres;
         a.mode = kEvalCertify;

@@ -52,7 +52,6 @@ struct alignas(16) SolveState {
     double inv_avg;
     Kkt best, kcert, kc, ka;
     unsigned arrive;           // CTA arrival counter of k_eval (re-armed by the last CTA)
-    unsigned err;              // set by a bounded wait that gave up
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -62,6 +61,9 @@ __device__ __forceinline__ unsigned long long global_ns() {
 }
 
 // ---------------------------------------------------------------- iteration kernels
+// Minimum resident CTAs per SM requested from the register allocator.
+template <class V>
+constexpr int kMinCtas = sizeof(V) == 4 ? 8 : 6;
 template <class M, class V>
 struct PrimalArgs {
     CsrView<M> AT;
@@ -77,40 +79,32 @@ struct PrimalArgs {
     const SolveState* st;
 };
 
-template <class V>
+template <class M, class V>
 struct PrimalEpi {
-    const V* __restrict__ x;
-    const V* __restrict__ c;
-    const V* __restrict__ l;
-    const V* __restrict__ u;
-    const V* __restrict__ qx;
-    V* __restrict__ xn;
-    V* __restrict__ xbar;
-    V* __restrict__ sumx;
+    const PrimalArgs<M, V>* a;  // kernel parameter space (__grid_constant__)
     V tau;
     struct Pre {
         V x, c, l, u, sumx, qx;
     };
     __device__ __forceinline__ Pre prefetch(int j) const {
-        return Pre{x[j], c[j], l[j], u[j], sumx[j], qx ? qx[j] : V(0)};
+        return Pre{a->x[j], a->c[j], a->l[j], a->u[j], a->sumx[j], a->qx ? a->qx[j] : V(0)};
     }
-    __device__ __forceinline__ void operator()(int j, const V (&s)[1], const Pre& p) {
+    __device__ __forceinline__ void operator()(int j, const V (&s)[1], const Pre& p) const {
         const V g = p.c - s[0] + p.qx;
         V v = p.x - tau * g;
         v = (v < p.l) ? p.l : v;
         v = (p.u < v) ? p.u : v;
-        xn[j] = v;
-        xbar[j] = V(2) * v - p.x;
-        sumx[j] = p.sumx + v;
+        a->xn[j] = v;
+        a->xbar[j] = V(2) * v - p.x;
+        a->sumx[j] = p.sumx + v;
     }
 };
 
 template <class M, class V>
-__global__ void __launch_bounds__(kThreads, sizeof(V) == 4 ? 4 : 2) k_primal(const PrimalArgs<M, V> a) {
+__global__ void __launch_bounds__(kThreads, kMinCtas<V>) k_primal(const __grid_constant__ PrimalArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    PrimalEpi<V> epi{a.x, a.c, a.l, a.u, a.qx, a.xn, a.xbar, a.sumx, static_cast<V>(a.st->tau)};
-    const CsrView<M> AT = a.AT;
-    spmv_run<1, M, V>(AT, blockIdx.x, GatherOne<V>{a.y}, epi, smem);
+    PrimalEpi<M, V> epi{&a, static_cast<V>(a.st->tau)};
+    spmv_run<1, M, V>(a.AT, blockIdx.x, GatherOne<V>{a.y}, epi, smem);
 }
 
 template <class M, class V>
@@ -125,36 +119,31 @@ struct DualArgs {
     const SolveState* st;
 };
 
-template <class V>
+template <class M, class V>
 struct DualEpi {
-    const V* __restrict__ y;
-    const V* __restrict__ lo;
-    const V* __restrict__ hi;
-    V* __restrict__ yn;
-    V* __restrict__ sumy;
+    const DualArgs<M, V>* a;  // kernel parameter space (__grid_constant__)
     V sigma;
     struct Pre {
         V y, lo, hi, sumy;
     };
-    __device__ __forceinline__ Pre prefetch(int i) const { return Pre{y[i], lo[i], hi[i], sumy[i]}; }
-    __device__ __forceinline__ void operator()(int i, const V (&s)[1], const Pre& p) {
+    __device__ __forceinline__ Pre prefetch(int i) const { return Pre{a->y[i], a->lo[i], a->hi[i], a->sumy[i]}; }
+    __device__ __forceinline__ void operator()(int i, const V (&s)[1], const Pre& p) const {
         const V q = p.y - sigma * s[0];
         const V l = sigma * p.lo, h = sigma * p.hi;
         V t = -q;
         t = (t < l) ? l : t;
         t = (h < t) ? h : t;
         const V v = q + t;
-        yn[i] = v;
-        sumy[i] = p.sumy + v;
+        a->yn[i] = v;
+        a->sumy[i] = p.sumy + v;
     }
 };
 
 template <class M, class V>
-__global__ void __launch_bounds__(kThreads, sizeof(V) == 4 ? 4 : 2) k_dual(const DualArgs<M, V> a) {
+__global__ void __launch_bounds__(kThreads, kMinCtas<V>) k_dual(const __grid_constant__ DualArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    DualEpi<V> epi{a.y, a.lo, a.hi, a.yn, a.sumy, static_cast<V>(a.st->sigma)};
-    const CsrView<M> A = a.A;
-    spmv_run<1, M, V>(A, blockIdx.x, GatherOne<V>{a.xbar}, epi, smem);
+    DualEpi<M, V> epi{&a, static_cast<V>(a.st->sigma)};
+    spmv_run<1, M, V>(a.A, blockIdx.x, GatherOne<V>{a.xbar}, epi, smem);
 }
 
 // ---------------------------------------------------------------- KKT evaluation
@@ -225,7 +214,7 @@ struct GatherYAvgRay {  // A^T side: y, ya and the ray y - yr
 // Per-row terms (backend_cpu.cpp:101-112, 132-142) and restart distances.
 template <class M, class V, int NV>
 struct EvalRowEpi {
-    EvalArgs<M, V> a;
+    const EvalArgs<M, V>& a;  // kernel parameter space (__grid_constant__)
     double inv;
     double t[kTerms];
     __device__ __forceinline__ static double pres2(double ax, double lo, double hi, double r) {
@@ -262,7 +251,7 @@ struct EvalRowEpi {
 // Per-column terms (backend_cpu.cpp:113-131, 143-149).
 template <class M, class V, int NV>
 struct EvalColEpi {
-    EvalArgs<M, V> a;
+    const EvalArgs<M, V>& a;  // kernel parameter space (__grid_constant__)
     double inv;
     double t[kTerms];
     __device__ __forceinline__ static void dres(double z, double lj, double uj, double cres, double& rd2,
@@ -404,11 +393,11 @@ static __device__ void decide(SolveState& s, const double (&T)[kTerms], int mode
 }
 
 template <class M, class V, int NVA, int NVT>
-__global__ void __launch_bounds__(kThreads) k_eval(const EvalArgs<M, V> a) {
+__global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double red[kWarps * kTerms];
     __shared__ bool am_last;
-    const int nctaA = a.A.ncta;
+    const int nctaA = a.A.nb;
     const double inv = (a.mode == kEvalCheck)
                            ? 1.0 / static_cast<double>(a.st->it_since + a.st->check_every)
                            : 0.0;
@@ -417,16 +406,14 @@ __global__ void __launch_bounds__(kThreads) k_eval(const EvalArgs<M, V> a) {
         EvalRowEpi<M, V, NVA> epi{a, inv, {}};
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) epi.t[k] = 0.0;
-        const CsrView<M> A = a.A;
-        spmv_run<NVA, M, V>(A, blockIdx.x, GatherXAvg<V, NVA>{a.x, a.sumx, inv}, epi, smem);
+        spmv_run<NVA, M, V>(a.A, blockIdx.x, GatherXAvg<V, NVA>{a.x, a.sumx, inv}, epi, smem);
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) t[k] = epi.t[k];
     } else {
         EvalColEpi<M, V, NVT> epi{a, inv, {}};
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) epi.t[k] = 0.0;
-        const CsrView<M> AT = a.AT;
-        spmv_run<NVT, M, V>(AT, blockIdx.x - nctaA, GatherYAvgRay<V, NVT>{a.y, a.sumy, a.yr, inv}, epi, smem);
+        spmv_run<NVT, M, V>(a.AT, blockIdx.x - nctaA, GatherYAvgRay<V, NVT>{a.y, a.sumy, a.yr, inv}, epi, smem);
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) t[k] = epi.t[k];
     }

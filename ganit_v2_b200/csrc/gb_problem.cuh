@@ -19,18 +19,13 @@ struct DevMat {
     DevBuf<float> val32;
     DevSchedule sched;
     std::vector<int> host_ptr;
-    unsigned* err = nullptr;  // device error flag (bounded waits)
-    // part: persistent partition (precision level 0..2)
     template <class M>
-    CsrView<M> view(int part) const {
+    CsrView<M> view() const {
         CsrView<M> v;
         v.ptr = ptr.get();
         v.idx = idx.get();
         v.val = val<M>();
         v.blocks = sched.blocks.get();
-        v.cta_start = sched.grid[part] > 0 ? sched.cta_start[part].get() : nullptr;
-        v.ncta = sched.ctas(part);
-        v.err = err;
         v.slots = sched.slots.get();
         v.counters = sched.counters.get();
         v.rows = rows;

@@ -25,14 +25,13 @@ struct Store2Epi {
 };
 // qx = Q x, qxa = Q xa (xa = inv * sumx)
 template <class M, class V>
-__global__ void __launch_bounds__(kThreads) k_spmv_q2(const CsrView<M> Q, const V* __restrict__ x,
+__global__ void __launch_bounds__(kThreads) k_spmv_q2(const __grid_constant__ CsrView<M> Q, const V* __restrict__ x,
                                                      const V* __restrict__ sumx, const SolveState* st,
                                                      V* __restrict__ qx, V* __restrict__ qxa) {
     extern __shared__ __align__(16) unsigned char smem[];
     const double inv = 1.0 / static_cast<double>(st->it_since + st->check_every);
     Store2Epi<V> epi{qx, qxa};
-    const CsrView<M> Qv = Q;
-    spmv_run<2, M, V>(Qv, blockIdx.x, GatherXAvg<V, 2>{x, sumx, inv}, epi, smem);
+    spmv_run<2, M, V>(Q, blockIdx.x, GatherXAvg<V, 2>{x, sumx, inv}, epi, smem);
 }
 
 // Partial F^T v for NV vectors: v0 = x, v1 = inv * sumx (when NV == 2).

@@ -73,12 +73,11 @@ struct StoreEpi {
     __device__ __forceinline__ void operator()(int r, const V (&s)[1], const NoPre&) { y[r] = s[0]; }
 };
 template <class M, class V>
-__global__ void __launch_bounds__(kThreads, sizeof(V) == 4 ? 4 : 2) k_spmv(const CsrView<M> A, const V* __restrict__ x,
-                                                     V* __restrict__ y) {
+__global__ void __launch_bounds__(kThreads) k_spmv(const __grid_constant__ CsrView<M> A, const V* __restrict__ x,
+                                                  V* __restrict__ y) {
     extern __shared__ __align__(16) unsigned char smem[];
     StoreEpi<V> epi{y};
-    const CsrView<M> Av = A;
-    spmv_run<1, M, V>(Av, blockIdx.x, GatherOne<V>{x}, epi, smem);
+    spmv_run<1, M, V>(A, blockIdx.x, GatherOne<V>{x}, epi, smem);
 }
 
 // ---------------------------------------------------------------- transpose / scaling kernels
