@@ -21,6 +21,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libganit_ref.so")
+DROPIN_SO = os.path.join(HERE, "_ref", "libganit_dropin.so")
 
 STATUS = {0: "OPTIMAL", 1: "PRIMAL_INFEASIBLE", 2: "ITERATION_LIMIT", 3: "TIME_LIMIT", 4: "NUMERICAL_ERROR"}
 PRECISION = {"double": 0, "mixed": 1, "dynamic": 2}
@@ -80,6 +81,9 @@ def build(ref: bool = True) -> None:
     targets = ["oracle"]
     if ref and os.path.isdir("/root/reference/src"):
         targets.append("ref")
+        lib = os.path.join(os.path.dirname(HERE), "ganit_v2_b200", "libganit_b200.so")
+        if os.path.exists(lib):
+            targets.append("dropin")
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 
@@ -199,6 +203,32 @@ def ref_solve(lp, threads: int | None = None, **opts) -> OracleResult:
            C.byref(o), C.byref(r), _p(x), _p(y))
     if rc != 0:
         raise RuntimeError("reference solve_pdhg_cpu threw")
+    return OracleResult(STATUS[r.status], r.pobj, r.dobj, r.rel_p, r.rel_d, r.rel_gap, r.iterations,
+                        r.fp32_iterations, r.l2_iterations, r.restarts, r.setup_s, r.solve_s, x, y)
+
+
+def dropin_available() -> bool:
+    return os.path.exists(DROPIN_SO)
+
+
+def dropin_solve(lp, **opts) -> OracleResult:
+    """The reference's unmodified run_pdhg (src/pdhg_impl.hpp) driving the B200
+    kernels through include/ganit_b200_backend.hpp (needs a GPU)."""
+    lib = _load(DROPIN_SO)
+    a = _arrays(lp)
+    o = _options(**opts)
+    r = _RefRes()
+    x = np.zeros(lp.n)
+    y = np.zeros(lp.m)
+    f = lib.dropin_solve_b200
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 8 + [C.c_double, C.c_int] + [C.c_void_p] * 3 + \
+                 [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    rc = f(lp.m, lp.n, _p(a["ptr"]), _p(a["idx"]), _p(a["val"]), _p(a["c"]), _p(a["l"]), _p(a["u"]), _p(a["lo"]),
+           _p(a["hi"]), float(lp.obj_const), int(lp.maximize), _p(a["qptr"]), _p(a["qidx"]), _p(a["qval"]),
+           C.byref(o), C.byref(r), _p(x), _p(y))
+    if rc != 0:
+        raise RuntimeError("run_pdhg with B200Backend threw")
     return OracleResult(STATUS[r.status], r.pobj, r.dobj, r.rel_p, r.rel_d, r.rel_gap, r.iterations,
                         r.fp32_iterations, r.l2_iterations, r.restarts, r.setup_s, r.solve_s, x, y)
 
