@@ -322,6 +322,70 @@ class Problem:
         self.close()
 
 
+class BatchSolver:
+    """Many independent LPs solved together on one GPU (gb_batch_*).
+
+    The batch is one block-diagonal problem: every instance keeps its own
+    scaling, step sizes, restarts, primal weight, precision phases and FP64
+    certification, exactly as if solved alone; a finished instance stops
+    costing bandwidth.  LPs only (no Hessian)."""
+
+    def __init__(self, lps, opt: Options | None = None):
+        self._lib = load_library()
+        self.lps = list(lps)
+        self._views = [_LpView(lp) for lp in self.lps]
+        arr = (_GbLp * len(self._views))(*[v.s for v in self._views])
+        o = _opts(opt)
+        h = C.c_void_p()
+        _check(self._lib.gb_batch_create(len(self._views), arr, C.addressof(o), C.byref(h)))
+        self._h = h
+
+    def __len__(self):
+        return len(self.lps)
+
+    def solve(self, opt: Options | None = None, fetch: bool = True) -> list:
+        o = _opts(opt)
+        res = (_GbResult * len(self.lps))()
+        _check(self._lib.gb_batch_solve(self._h, C.addressof(o), res))
+        out = []
+        for i, r in enumerate(res):
+            x = y = None
+            if fetch:
+                x, y = self.solution(i)
+            out.append(_result(r, x, y))
+        return out
+
+    def solution(self, i: int):
+        lp = self.lps[i]
+        x = np.zeros(lp.n)
+        y = np.zeros(lp.m)
+        _check(self._lib.gb_batch_get_solution(self._h, int(i), _p(x), _p(y)))
+        return x, y
+
+    def schedule(self) -> dict:
+        t, b = C.c_int(), C.c_int()
+        g = np.zeros(2 * len(self.lps), dtype=np.int32)
+        _check(self._lib.gb_batch_schedule(self._h, C.byref(t), C.byref(b), _p(g)))
+        return {"threads": t.value, "blocks_per_sm": b.value, "groups_A": g[0::2].copy(), "groups_AT": g[1::2].copy()}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.gb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
 # ---------------------------------------------------------------- Backend concept
 class Vec:
     def __init__(self, be: "Backend", h):

@@ -1,13 +1,16 @@
-// Single-problem engine and the C ABI (include/ganit_b200.h).
+// Engine for a resident batch of problems and the C ABI of the fused solver
+// (include/ganit_b200.h).  One problem is a batch of one.
 //
 // gb_solve / gb_problem_*  : restarted PDHG with every step on the device
 //                            (replaces ganit::solve_pdhg_gpu, backend_cuda.cu:382-393)
-// gb_backend_* / gb_vec_*  : the Backend concept ops that src/pdhg_impl.hpp
-//                            drives (replaces CudaBackend, backend_cuda.cu:286-378)
+// gb_batch_*               : many independent LPs as one block-diagonal problem,
+//                            each instance with its own scaling, step sizes,
+//                            restarts, primal weight, phases and certification
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <numeric>
 
 #include "gb_problem.cuh"
 #include "gb_qp.cuh"
@@ -45,7 +48,7 @@ inline void check_device(int dev, int* sms) {
     *sms = prop.multiProcessorCount;
 }
 
-// Opt every SpMV-based kernel into the dynamic shared memory it needs.
+// Opt a kernel into the dynamic shared memory it needs.
 template <class K>
 void set_smem(K kernel, size_t bytes) {
     GB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
@@ -55,7 +58,7 @@ void validate_lp(const gb_lp* lp) {
     GB_REQUIRE(lp != nullptr, "lp is NULL");
     GB_REQUIRE(lp->m > 0 && lp->n > 0, "need m > 0 and n > 0");
     GB_REQUIRE(lp->a_ptr && lp->c && lp->l && lp->u, "missing A/c/l/u");
-    GB_REQUIRE(lp->m == 0 || (lp->lo && lp->hi), "missing lo/hi");
+    GB_REQUIRE(lp->lo && lp->hi, "missing lo/hi");
     GB_REQUIRE(lp->a_ptr[0] == 0, "A.ptr[0] must be 0");
     for (int i = 0; i < lp->m; ++i) GB_REQUIRE(lp->a_ptr[i + 1] >= lp->a_ptr[i], "A.ptr must be nondecreasing");
     const long long nnz = lp->a_ptr[lp->m];
@@ -84,8 +87,6 @@ void upload_mat(DevMat& M, int rows, int cols, const int* ptr, const int* idx, c
     M.ptr.upload(ptr, rows + 1, s);
     M.idx.reset(padded_nnz(M.nnz));
     M.val64.reset(padded_nnz(M.nnz));
-    GB_CUDA(cudaMemsetAsync(M.idx.get(), 0, M.idx.size() * sizeof(int), s));
-    GB_CUDA(cudaMemsetAsync(M.val64.get(), 0, M.val64.size() * sizeof(double), s));
     if (M.nnz) {
         M.idx.upload(idx, M.nnz, s);
         M.val64.upload(val, M.nnz, s);
@@ -104,10 +105,8 @@ void device_transpose(Problem& P, cudaStream_t s) {
     P.AT.ptr.reset(n + 1);
     P.AT.idx.reset(padded_nnz(nnz));
     P.AT.val64.reset(padded_nnz(nnz));
-    GB_CUDA(cudaMemsetAsync(P.AT.idx.get(), 0, P.AT.idx.size() * sizeof(int), s));
-    GB_CUDA(cudaMemsetAsync(P.AT.val64.get(), 0, P.AT.val64.size() * sizeof(double), s));
     const int g = elem_grid(std::max(nnz, m * 32), P.sms);
-    if (m) k_row_of<<<g, kThreads, 0, s>>>(m, P.A.ptr.get(), P.row_of.get());
+    k_row_of<<<g, kThreads, 0, s>>>(m, P.A.ptr.get(), P.row_of.get());
     DevBuf<int> cnt(n + 1), keys_out, iota;
     DevBuf<unsigned char> tmp;
     GB_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int) * (n + 1), s));
@@ -136,72 +135,53 @@ void device_transpose(Problem& P, cudaStream_t s) {
     GB_CUDA(cudaStreamSynchronize(s));
 }
 
-__global__ void k_finish_norms(double* sc, int empty) {
-    // sc[2] = sqrt(lambda) * 1.01, or 1 for an empty matrix (scaling.cpp:132, 153-154)
-    sc[2] = empty ? 1.0 : sqrt(sc[8]) * 1.01;
-}
-__global__ void k_finish_normq(double* sc) { sc[3] = sc[8] * 1.01; }  // scaling.cpp:124
-__global__ void k_w0(double* sc, const double* cn, const double* bn) {
-    // w0 = ||c'|| / ||b'||_finite (pdhg_impl.hpp:258-261)
-    const double c = *cn, b = *bn;
-    sc[6] = (c > 1e-10 && b > 1e-10) ? c / b : 1.0;
+// Per-instance fixed-order reduction into scal[k][slot]: rows (m) or columns (n).
+template <class F, class Post>
+void inst_reduce(Problem& P, bool rows, F f, int slot, Post post, cudaStream_t s) {
+    if (P.count == 1) {
+        reduce_to(s, rows ? P.m : P.n, f, P.red_partials.get(), P.scal.get() + slot, post);
+    } else {
+        k_seg_red<F, Post><<<P.count, kThreads, 0, s>>>(rows ? P.d_row_off.get() : P.d_col_off.get(), f,
+                                                      P.scal.get() + slot, post);
+    }
 }
 
-// Power iteration on the scaled data (scaling.cpp:131-155 for A'^T A',
-// scaling.cpp:108-124 for Q').  ||A'|| lands in P.scal[2].
-void power_norm_A(Problem& P, cudaStream_t s) {
-    const int n = P.n;
-    double* pw = P.scal.get() + 7;  // [0] norm, [1] lambda, [2] stopped
-    GB_CUDA(cudaMemsetAsync(pw, 0, 3 * sizeof(double), s));
-    if (P.A.nnz == 0) {
-        k_finish_norms<<<1, 1, 0, s>>>(P.scal.get(), 1);
-        return;
-    }
-    double* v = P.x64.get();  // reuse FP64 vectors as scratch before the solve
-    double* w = P.work2.get();
-    double* z = P.work1.get();
-    k_fill<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, 1.0, v);
-    reduce_to(s, n, Sq{v}, P.red_partials.get(), pw, PostSqrt{});
-    k_power_step<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, v, v, pw);  // v /= ||v|| (lambda overwritten below)
-    GB_CUDA(cudaMemsetAsync(pw + 1, 0, 2 * sizeof(double), s));
-    const size_t sm1 = spmv_smem_bytes<1, double>();
-    for (int it = 0; it < 50; ++it) {
-        k_spmv<double, double><<<P.A.sched.nb, kThreads, sm1, s>>>(P.A.view<double>(), v, w);
-        k_spmv<double, double><<<P.AT.sched.nb, kThreads, sm1, s>>>(P.AT.view<double>(), w, z);
-        reduce_to(s, n, Sq{z}, P.red_partials.get(), pw, PostSqrt{});
-        k_power_step<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, z, v, pw);
-    }
-    k_finish_norms<<<1, 1, 0, s>>>(P.scal.get(), 0);
-}
-
+// Power iteration on the scaled data, per instance (scaling.cpp:131-155 for
+// A'^T A', scaling.cpp:108-124 for Q').
 void qx_dplr_f64(Problem& P, const double* x, double* out, cudaStream_t s);
 
-void power_norm_Q(Problem& P, cudaStream_t s) {
+void power_iteration(Problem& P, bool q, cudaStream_t s) {
     const int n = P.n;
-    double* pw = P.scal.get() + 7;
-    double* v = P.x64.get();
-    double* w = P.work1.get();
-    GB_CUDA(cudaMemsetAsync(pw, 0, 3 * sizeof(double), s));
+    double* v = P.x64.get();  // FP64 vectors double as scratch before the solve
+    double* w = P.work2.get();
+    double* z = P.work1.get();
+    double* sc = P.scal.get();
+    const int gi = div_up(P.count, kThreads);
     k_fill<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, 1.0, v);
-    reduce_to(s, n, Sq{v}, P.red_partials.get(), pw, PostSqrt{});
-    k_power_step<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, v, v, pw);
-    GB_CUDA(cudaMemsetAsync(pw + 1, 0, 2 * sizeof(double), s));
+    inst_reduce(P, false, Sq{v}, S_PW_NORM, PostSqrt{}, s);
+    k_power_reset<<<gi, kThreads, 0, s>>>(P.count, sc);
+    k_power_vec<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, P.icol(), sc, v, v);  // v /= ||v||
     const size_t sm1 = spmv_smem_bytes<1, double>();
-    for (int it = 0; it < 60; ++it) {
-        if (P.dplr)
-            qx_dplr_f64(P, v, w, s);
-        else
-            k_spmv<double, double><<<P.Q.sched.nb, kThreads, sm1, s>>>(P.Q.view<double>(), v, w);
-        reduce_to(s, n, Sq{w}, P.red_partials.get(), pw, PostSqrt{});
-        k_power_step<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, w, v, pw);
+    const int iters = q ? 60 : 50;
+    for (int it = 0; it < iters; ++it) {
+        if (q) {
+            if (P.dplr) qx_dplr_f64(P, v, z, s);
+            else k_spmv<double, double><<<P.Q.sched.nb, kThreads, sm1, s>>>(P.Q.view<double>(), v, z);
+        } else {
+            k_spmv<double, double><<<P.A.sched.nb, kThreads, sm1, s>>>(P.A.view<double>(), v, w);
+            k_spmv<double, double><<<P.AT.sched.nb, kThreads, sm1, s>>>(P.AT.view<double>(), w, z);
+        }
+        inst_reduce(P, false, Sq{z}, S_PW_NORM, PostSqrt{}, s);
+        k_power_vec<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, P.icol(), sc, z, v);
+        k_power_flags<<<gi, kThreads, 0, s>>>(P.count, sc);
     }
-    k_finish_normq<<<1, 1, 0, s>>>(P.scal.get());
+    k_finish_norms<<<gi, kThreads, 0, s>>>(P.count, P.d_nnz_off.get(), sc, q ? 1 : 0);
 }
 
-// DPLR product in FP64 used by the setup power iteration (st == nullptr: one vector).
+// DPLR product in FP64 used by the setup power iteration.
 void qx_dplr_f64(Problem& P, const double* x, double* out, cudaStream_t s) {
     double* part = P.partials.get();
-    double* t = P.v64.ftx.get();
+    double* t = P.ftx.get();
     k_ftx_partial<double, 1><<<kFtxGrid, kThreads, 0, s>>>(P.n, P.qk, P.F64.get(), x, nullptr, nullptr, part);
     k_ftx_final<<<1, kThreads, 0, s>>>(kFtxGrid, P.qk, part, t);
     k_dplr_expand<double, 1><<<elem_grid((long long)P.n * 32, P.sms), kThreads, 0, s>>>(
@@ -239,9 +219,20 @@ void init_kernel_attrs() {
     });
 }
 
-// Upload + device setup (scale_lp + estimate_norm + run_pdhg's start point).
-Problem* create_problem(const gb_lp* lp, const gb_options* opt) {
-    validate_lp(lp);
+// Instance index of every element of [0, off[count]).
+__global__ void k_fill_segments(const int* off, int* out) {
+    const int k = blockIdx.x;
+    for (int i = off[k] + threadIdx.x; i < off[k + 1]; i += blockDim.x) out[i] = k;
+}
+
+// Upload + device setup (scale_lp + estimate_norm + run_pdhg's start point)
+// of `count` instances.
+Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
+    GB_REQUIRE(count >= 1 && lps != nullptr, "need at least one problem");
+    for (int k = 0; k < count; ++k) validate_lp(&lps[k]);
+    if (count > 1)
+        for (int k = 0; k < count; ++k)
+            GB_REQUIRE(lps[k].q_ptr == nullptr && lps[k].q_rank == 0, "batched solving takes LPs only (no Hessian)");
     auto P = std::make_unique<Problem>();
     P->device = g_device;
     GB_CUDA(cudaSetDevice(P->device));
@@ -250,54 +241,118 @@ Problem* create_problem(const gb_lp* lp, const gb_options* opt) {
     GB_CUDA(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
     cudaStream_t s = P->stream;
     const auto t0 = std::chrono::steady_clock::now();
-    const int m = lp->m, n = lp->n;
+    P->count = count;
+    P->row_off.assign(count + 1, 0);
+    P->col_off.assign(count + 1, 0);
+    P->nnz_off.assign(count + 1, 0);
+    P->maximize.resize(count);
+    P->obj_const.resize(count);
+    for (int k = 0; k < count; ++k) {
+        P->row_off[k + 1] = P->row_off[k] + lps[k].m;
+        P->col_off[k + 1] = P->col_off[k] + lps[k].n;
+        const long long z = static_cast<long long>(P->nnz_off[k]) + lps[k].a_ptr[lps[k].m];
+        GB_REQUIRE(z < (1LL << 31) - 16, "more than 2^31 nonzeros in one problem");
+        P->nnz_off[k + 1] = static_cast<int>(z);
+        P->maximize[k] = lps[k].maximize != 0;
+        P->obj_const[k] = lps[k].obj_const;
+    }
+    const int m = P->row_off[count], n = P->col_off[count];
     P->m = m;
     P->n = n;
-    P->maximize = lp->maximize != 0;
-    P->obj_const = lp->obj_const;
-    const double sign = P->maximize ? -1.0 : 1.0;
 
-    upload_mat(P->A, m, n, lp->a_ptr, lp->a_idx, lp->a_val, s);
+    // Host layout of the block-diagonal problem (a single problem is used in place).
+    std::vector<int> hptr, hidx;
+    std::vector<double> hval, hc, hl, hu, hlo, hhi;
+    const int *ap = lps[0].a_ptr, *ai = lps[0].a_idx;
+    const double *av = lps[0].a_val, *vc = lps[0].c, *vl = lps[0].l, *vu = lps[0].u, *vlo = lps[0].lo,
+                 *vhi = lps[0].hi;
+    if (count > 1) {
+        hptr.resize(m + 1);
+        hidx.resize(P->nnz_off[count]);
+        hval.resize(P->nnz_off[count]);
+        for (auto* v : {&hc, &hl, &hu}) v->resize(n);
+        for (auto* v : {&hlo, &hhi}) v->resize(m);
+        for (int k = 0; k < count; ++k) {
+            const gb_lp& L = lps[k];
+            const int r0 = P->row_off[k], c0 = P->col_off[k], z0 = P->nnz_off[k];
+            for (int i = 0; i <= L.m; ++i) hptr[r0 + i] = z0 + L.a_ptr[i];
+            const int nz = L.a_ptr[L.m];
+            for (int p = 0; p < nz; ++p) {
+                hidx[z0 + p] = c0 + L.a_idx[p];
+                hval[z0 + p] = L.a_val[p];
+            }
+            std::copy(L.c, L.c + L.n, hc.begin() + c0);
+            std::copy(L.l, L.l + L.n, hl.begin() + c0);
+            std::copy(L.u, L.u + L.n, hu.begin() + c0);
+            std::copy(L.lo, L.lo + L.m, hlo.begin() + r0);
+            std::copy(L.hi, L.hi + L.m, hhi.begin() + r0);
+        }
+        ap = hptr.data(); ai = hidx.data(); av = hval.data();
+        vc = hc.data(); vl = hl.data(); vu = hu.data(); vlo = hlo.data(); vhi = hhi.data();
+    }
+    auto upi = [&](DevBuf<int>& d, const std::vector<int>& h) {
+        d.reset(h.size());
+        d.upload(h.data(), h.size(), s);
+    };
+    upi(P->d_row_off, P->row_off);
+    upi(P->d_col_off, P->col_off);
+    upi(P->d_nnz_off, P->nnz_off);
+    if (count > 1) {
+        P->inst_row.reset(m);
+        P->inst_col.reset(n);
+        k_fill_segments<<<count, kThreads, 0, s>>>(P->d_row_off.get(), P->inst_row.get());
+        k_fill_segments<<<count, kThreads, 0, s>>>(P->d_col_off.get(), P->inst_col.get());
+    }
+
+    upload_mat(P->A, m, n, ap, ai, av, s);
     auto up = [&](DevBuf<double>& d, const double* h, int k) {
         d.reset(k ? k : 1);
         d.upload(h, k, s);
     };
     DevBuf<double> c0, l0, u0, lo0, hi0;
-    up(c0, lp->c, n);
-    up(l0, lp->l, n);
-    up(u0, lp->u, n);
-    up(lo0, lp->lo, m);
-    up(hi0, lp->hi, m);
+    up(c0, vc, n);
+    up(l0, vl, n);
+    up(u0, vu, n);
+    up(lo0, vlo, m);
+    up(hi0, vhi, m);
     for (DevBuf<double>* b : {&P->c, &P->l, &P->u, &P->C, &P->Cres, &P->x64, &P->xr64, &P->xo, &P->work1})
-        b->reset(n ? n : 1);
-    for (DevBuf<double>* b : {&P->lo, &P->hi, &P->R, &P->Rres, &P->y64, &P->yr64, &P->yo, &P->work2})
-        b->reset(m ? m : 1);
-    P->scal.reset(16);
-    GB_CUDA(cudaMemsetAsync(P->scal.get(), 0, 16 * sizeof(double), s));
+        b->reset(n);
+    for (DevBuf<double>* b : {&P->lo, &P->hi, &P->R, &P->Rres, &P->y64, &P->yr64, &P->yo, &P->work2}) b->reset(m);
+    P->scal.reset(static_cast<size_t>(count) * kScal);
+    P->scal_host.assign(static_cast<size_t>(count) * kScal, 0.0);
+    for (int k = 0; k < count; ++k) {
+        P->scal_host[static_cast<size_t>(k) * kScal + S_SIGN] = P->maximize[k] ? -1.0 : 1.0;
+        P->scal_host[static_cast<size_t>(k) * kScal + S_OBJC] = (P->maximize[k] ? -1.0 : 1.0) * P->obj_const[k];
+    }
+    P->scal.upload(P->scal_host.data(), P->scal_host.size(), s);
     P->red_partials.reset(kRedGrid);
+    P->st.reset(count);
+    GB_CUDA(cudaMemsetAsync(P->st.get(), 0, sizeof(SolveState) * count, s));
+    P->arrive.reset(1);
+    GB_CUDA(cudaMemsetAsync(P->arrive.get(), 0, sizeof(unsigned), s));
 
-    // schedules (host, from the row-length histogram) and transpose
-        P->st.reset(1);
-    GB_CUDA(cudaMemsetAsync(P->st.get(), 0, sizeof(SolveState), s));
-    P->A.sched.upload(build_schedule(P->A.host_ptr.data(), m), 3, s);
+    // schedules (host, from the row-length histogram, per instance) and transpose
+    P->A.sched.upload(build_schedule(P->A.host_ptr.data(), m, P->row_off.data(), count), 3, s);
     device_transpose(*P, s);
-    P->AT.sched.upload(build_schedule(P->AT.host_ptr.data(), n), 3, s);
+    P->AT.sched.upload(build_schedule(P->AT.host_ptr.data(), n, P->col_off.data(), count), 3, s);
 
-    // Ruiz equilibration + Pock-Chambolle (scaling.cpp:47-72)
+    // Ruiz equilibration + Pock-Chambolle (scaling.cpp:47-72); row and column
+    // factors are per row / column, so the block-diagonal matrix scales every
+    // instance exactly as it would alone.
     const int gw = elem_grid(static_cast<long long>(std::max(m, n)) * 32, P->sms);
     const int ge = elem_grid(std::max<long long>(P->A.nnz, 1), P->sms);
-    DevBuf<double> rs(m ? m : 1), cs(n);
+    DevBuf<double> rs(m), cs(n);
     k_fill<<<elem_grid(m, P->sms), kThreads, 0, s>>>(m, 1.0, P->R.get());
     k_fill<<<elem_grid(n, P->sms), kThreads, 0, s>>>(n, 1.0, P->C.get());
     const int passes = opt->ruiz_iters + (opt->pock_chambolle ? 1 : 0);
     for (int it = 0; it < passes; ++it) {
         const int mode = it < opt->ruiz_iters ? 0 : 1;
-        if (m) k_row_norm_factor<<<gw, kThreads, 0, s>>>(m, P->A.ptr.get(), nullptr, P->A.val64.get(), mode, rs.get());
+        k_row_norm_factor<<<gw, kThreads, 0, s>>>(m, P->A.ptr.get(), nullptr, P->A.val64.get(), mode, rs.get());
         k_row_norm_factor<<<gw, kThreads, 0, s>>>(n, P->AT.ptr.get(), P->perm.get(), P->A.val64.get(), mode, cs.get());
         if (P->A.nnz)
             k_apply_scaling<<<ge, kThreads, 0, s>>>(static_cast<int>(P->A.nnz), P->row_of.get(), P->A.idx.get(),
                                                     rs.get(), cs.get(), P->A.val64.get());
-        if (m) k_mul_into<<<elem_grid(m, P->sms), kThreads, 0, s>>>(m, rs.get(), P->R.get());
+        k_mul_into<<<elem_grid(m, P->sms), kThreads, 0, s>>>(m, rs.get(), P->R.get());
         k_mul_into<<<elem_grid(n, P->sms), kThreads, 0, s>>>(n, cs.get(), P->C.get());
     }
     if (P->A.nnz)
@@ -305,52 +360,51 @@ Problem* create_problem(const gb_lp* lp, const gb_options* opt) {
                                                   P->A.val64.get(), P->AT.idx.get(), P->AT.val64.get());
     // vectors (scaling.cpp:75-101)
     const int gv = elem_grid(std::max(m, n), P->sms);
-    k_scale_vectors<<<gv, kThreads, 0, s>>>(n, m, sign, c0.get(), l0.get(), u0.get(), lo0.get(), hi0.get(),
+    double* sc = P->scal.get();
+    k_scale_vectors<<<gv, kThreads, 0, s>>>(n, m, P->icol(), sc, c0.get(), l0.get(), u0.get(), lo0.get(), hi0.get(),
                                             P->R.get(), P->C.get(), P->c.get(), P->l.get(), P->u.get(), P->lo.get(),
                                             P->hi.get());
-    double* sc = P->scal.get();
-    reduce_to(s, m, FiniteBoundSq{P->lo.get(), P->hi.get()}, P->red_partials.get(), sc + 0, PostSqrtPlus1{});
-    reduce_to(s, n, Sq{P->c.get()}, P->red_partials.get(), sc + 1, PostSqrtPlus1{});
-    k_rescale<<<gv, kThreads, 0, s>>>(n, m, sc, P->R.get(), P->C.get(), P->c.get(), P->l.get(), P->u.get(),
-                                      P->lo.get(), P->hi.get(), P->Rres.get(), P->Cres.get());
+    inst_reduce(*P, true, FiniteBoundSq{P->lo.get(), P->hi.get()}, S_BSCALE, PostSqrtPlus1{}, s);
+    inst_reduce(*P, false, Sq{P->c.get()}, S_CSCALE, PostSqrtPlus1{}, s);
+    k_rescale<<<gv, kThreads, 0, s>>>(n, m, P->icol(), P->irow(), sc, P->R.get(), P->C.get(), P->c.get(), P->l.get(),
+                                      P->u.get(), P->lo.get(), P->hi.get(), P->Rres.get(), P->Cres.get());
     // norms of the ORIGINAL data (scaling.cpp:126-127)
-    reduce_to(s, m, FiniteBoundSq{lo0.get(), hi0.get()}, P->red_partials.get(), sc + 4, PostSqrt{});
-    reduce_to(s, n, Sq{c0.get()}, P->red_partials.get(), sc + 5, PostSqrt{});
+    inst_reduce(*P, true, FiniteBoundSq{lo0.get(), hi0.get()}, S_BNORM, PostSqrt{}, s);
+    inst_reduce(*P, false, Sq{c0.get()}, S_CNORM, PostSqrt{}, s);
 
-    // Hessian
-    P->has_q = (lp->q_ptr && lp->q_ptr[n] > 0) || lp->q_rank > 0;
-    P->dplr = lp->q_rank > 0;
-    P->qk = P->dplr ? lp->q_rank : 0;
+    // Hessian (single problem only)
+    const gb_lp& L0 = lps[0];
+    P->has_q = count == 1 && ((L0.q_ptr && L0.q_ptr[n] > 0) || L0.q_rank > 0);
+    P->dplr = P->has_q && L0.q_rank > 0;
+    P->qk = P->dplr ? L0.q_rank : 0;
     P->partials.reset(std::max<size_t>(static_cast<size_t>(kFtxGrid) * 2 * kMaxRank,
                                        static_cast<size_t>(P->A.sched.nb + P->AT.sched.nb) * kTerms));
+    P->ftx.reset(2 * kMaxRank);
     P->v32.alloc(n, m, P->qk, P->has_q);
     P->v64.alloc(n, m, P->qk, P->has_q);
     if (P->has_q && !P->dplr) {
-        upload_mat(P->Q, n, n, lp->q_ptr, lp->q_idx, lp->q_val, s);
+        upload_mat(P->Q, n, n, L0.q_ptr, L0.q_idx, L0.q_val, s);
         P->Q.sched.upload(build_schedule(P->Q.host_ptr.data(), n), 3, s);
         P->q_row_of.reset(P->Q.nnz ? P->Q.nnz : 1);
         k_row_of<<<elem_grid((long long)n * 32, P->sms), kThreads, 0, s>>>(n, P->Q.ptr.get(), P->q_row_of.get());
         k_scale_q<<<elem_grid(P->Q.nnz, P->sms), kThreads, 0, s>>>(static_cast<int>(P->Q.nnz), P->q_row_of.get(),
-                                                                 P->Q.idx.get(), sign, P->C.get(), sc,
-                                                                 P->Q.val64.get());
+                                                                 P->Q.idx.get(), P->C.get(), sc, P->Q.val64.get());
     } else if (P->dplr) {
         P->F64.reset(static_cast<size_t>(n) * P->qk);
-        P->F64.upload(lp->q_F, static_cast<size_t>(n) * P->qk, s);
-        up(P->D64, lp->q_D, n);
+        P->F64.upload(L0.q_F, static_cast<size_t>(n) * P->qk, s);
+        up(P->D64, L0.q_D, n);
         k_scale_dplr<<<elem_grid((long long)n * P->qk, P->sms), kThreads, 0, s>>>(n, P->qk, P->C.get(), sc,
                                                                                   P->F64.get(), P->D64.get());
     }
-    if (P->has_q) power_norm_Q(*P, s);
-    // ||A'|| (scaling.cpp:131-155)
-    power_norm_A(*P, s);
+    if (P->has_q) power_iteration(*P, true, s);
+    power_iteration(*P, false, s);  // ||A'|| (scaling.cpp:131-155)
     // w0 from the scaled data (pdhg_impl.hpp:258-261)
-    reduce_to(s, n, Sq{P->c.get()}, P->red_partials.get(), sc + 10, PostSqrt{});
-    reduce_to(s, m, FiniteBoundSq{P->lo.get(), P->hi.get()}, P->red_partials.get(), sc + 11, PostSqrt{});
-    k_w0<<<1, 1, 0, s>>>(sc, sc + 10, sc + 11);
+    inst_reduce(*P, false, Sq{P->c.get()}, S_CN, PostSqrt{}, s);
+    inst_reduce(*P, true, FiniteBoundSq{P->lo.get(), P->hi.get()}, S_BN, PostSqrt{}, s);
+    k_w0<<<div_up(count, kThreads), kThreads, 0, s>>>(count, sc);
     // FP32 copies of the matrix values and data
     auto cvt32 = [&](DevMat& M) {
         M.val32.reset(padded_nnz(M.nnz));
-        GB_CUDA(cudaMemsetAsync(M.val32.get(), 0, M.val32.size() * sizeof(float), s));
         if (M.nnz) k_convert<float><<<elem_grid(M.nnz, P->sms), kThreads, 0, s>>>(M.nnz, M.val64.get(), M.val32.get());
     };
     cvt32(P->A);
@@ -358,8 +412,10 @@ Problem* create_problem(const gb_lp* lp, const gb_options* opt) {
     if (P->has_q && !P->dplr) cvt32(P->Q);
     convert_data(*P, P->v32, s);
     convert_data(*P, P->v64, s);
-    GB_CUDA(cudaMallocHost(&P->st_host, sizeof(SolveState)));
-    GB_CUDA(cudaMemcpyAsync(P->scal_host, sc, 10 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaMallocHost(&P->st_host, sizeof(SolveState) * count));
+    GB_CUDA(cudaMallocHost(&P->phase_flags_host, sizeof(int) * count));
+    P->phase_flags.reset(count);
+    GB_CUDA(cudaMemcpyAsync(P->scal_host.data(), sc, sizeof(double) * P->scal_host.size(), cudaMemcpyDeviceToHost, s));
     GB_CUDA(cudaStreamSynchronize(s));
     GB_CUDA(cudaGetLastError());
     P->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -386,7 +442,7 @@ template <class M, class V>
 void launch_qx(Problem& P, VecSet<V>& vs, const V* x, V* qx, cudaStream_t s, long long& nl) {
     if (P.dplr) {
         double* part = P.partials.get();
-        double* t = P.v64.ftx.get();  // FP64 F^T x of any level
+        double* t = P.ftx.get();  // FP64 F^T x at every level
         k_ftx_partial<V, 1><<<kFtxGrid, kThreads, 0, s>>>(P.n, P.qk, vs.F.get(), x, nullptr, nullptr, part);
         k_ftx_final<<<1, kThreads, 0, s>>>(kFtxGrid, P.qk, part, t);
         k_dplr_expand<V, 1><<<elem_grid((long long)P.n * 32, P.sms), kThreads, 0, s>>>(
@@ -402,7 +458,7 @@ template <class M, class V>
 void launch_qx2(Problem& P, VecSet<V>& vs, const V* x, cudaStream_t s, long long& nl) {
     if (P.dplr) {
         double* part = P.partials.get();
-        double* t = P.v64.ftx.get();
+        double* t = P.ftx.get();
         k_ftx_partial<V, 2><<<kFtxGrid, kThreads, 0, s>>>(P.n, P.qk, vs.F.get(), x, vs.sumx.get(), P.st.get(), part);
         k_ftx_final<<<1, kThreads, 0, s>>>(kFtxGrid, 2 * P.qk, part, t);
         k_dplr_expand<V, 2><<<elem_grid((long long)P.n * 32, P.sms), kThreads, 0, s>>>(
@@ -436,7 +492,11 @@ EvalArgs<M, V> eval_args(Problem& P, VecSet<V>& vs, const V* x, const V* y, int 
     a.qx = with_q ? vs.qx.get() : nullptr;
     a.qxa = (with_q && mode == kEvalCheck) ? vs.qxa.get() : nullptr;
     a.mode = mode;
+    a.count = P.count;
+    a.seg_a = P.A.sched.seg_block.get();
+    a.seg_t = P.AT.sched.seg_block.get();
     a.st = P.st.get();
+    a.arrive = P.arrive.get();
     a.partials = P.partials.get();
     a.cond = 0;
     a.use_cond = 0;
@@ -445,7 +505,7 @@ EvalArgs<M, V> eval_args(Problem& P, VecSet<V>& vs, const V* x, const V* y, int 
 
 // One PDHG iteration (k-th inside the body) on buffers selected by parity.
 template <class M, class V>
-void launch_iteration(Problem& P, VecSet<V>& vs, int k, cudaStream_t s, long long& nl) {
+void launch_iteration(Problem& P, VecSet<V>& vs, int k, cudaStream_t s, long long& nl, cudaEvent_t mid = nullptr) {
     const V* xin = (k & 1) ? vs.x1.get() : vs.x0.get();
     V* xout = (k & 1) ? vs.x0.get() : vs.x1.get();
     const V* yin = (k & 1) ? vs.y1.get() : vs.y0.get();
@@ -455,6 +515,7 @@ void launch_iteration(Problem& P, VecSet<V>& vs, int k, cudaStream_t s, long lon
     PrimalArgs<M, V> pa{P.AT.view<M>(), yin, xin, vs.c.get(), vs.l.get(), vs.u.get(),
                         P.has_q ? vs.qx.get() : nullptr, xout, vs.xbar.get(), vs.sumx.get(), P.st.get()};
     k_primal<M, V><<<P.AT.sched.nb, kThreads, sm, s>>>(pa);
+    if (mid) GB_CUDA(cudaEventRecord(mid, s));
     DualArgs<M, V> da{P.A.view<M>(), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(),
                       P.st.get()};
     k_dual<M, V><<<P.A.sched.nb, kThreads, sm, s>>>(da);
@@ -478,7 +539,7 @@ long long capture_body(Problem& P, int ce, cudaGraphConditionalHandle cond, cuda
     const int grid = P.A.sched.nb + P.AT.sched.nb;
     k_eval<M, V, 2, 3><<<grid, kThreads, spmv_smem_bytes<3, V>(), s>>>(ea);
     RestartArgs<V> ra{xc, yc, vs.x0.get(), vs.y0.get(), vs.xr.get(), vs.yr.get(), vs.sumx.get(), vs.sumy.get(),
-                      P.n, P.m, P.st.get()};
+                      P.n, P.m, P.icol(), P.irow(), P.st.get()};
     k_restart<V><<<elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s>>>(ra);
     nl += 2;
     return nl;
@@ -533,25 +594,37 @@ bool host_loop_mode() {
     return host;
 }
 
-__global__ void k_set_phase(SolveState* st, double tol, int stall_checks, int stall_exit, int first_phase) {
-    st->phase_tol = tol;
-    st->stall_checks = stall_checks;
-    st->stall_exit = stall_exit;
-    st->carry_restart_err = first_phase ? -1.0 : st->restart_err;
+// Phase set-up of every instance: in_phase / active from flags.
+__global__ void k_set_phase(int count, SolveState* st, const int* flags, double tol, int stall_checks,
+                            int stall_exit, int first_phase) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    SolveState& s = st[k];
+    s.in_phase = flags[k];
+    s.active = flags[k];
+    s.ran_body = 0;
+    if (!flags[k]) return;
+    s.phase_tol = tol;
+    s.stall_checks = stall_checks;
+    s.stall_exit = stall_exit;
+    s.carry_restart_err = first_phase ? -1.0 : s.restart_err;
 }
 
-__global__ void k_init_state(SolveState* st, const double* sc, double obj_const, int has_q, int check_every,
+__global__ void k_init_state(int count, SolveState* st, const double* sc, int has_q, int check_every,
                              long long max_iter, double time_limit, double infeas_tol) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const double* s0 = sc + static_cast<size_t>(k) * kScal;
     SolveState s;
     memset(&s, 0, sizeof(s));
-    s.normA = sc[2];
+    s.normA = s0[S_NORMA];
     s.eta = 0.998 / s.normA;
-    s.normQ = sc[3];
-    s.obj_scale = sc[1] * sc[0];
-    s.obj_const = obj_const;
-    s.bnorm = sc[4];
-    s.cnorm = sc[5];
-    s.w = sc[6];
+    s.normQ = s0[S_NORMQ];
+    s.obj_scale = s0[S_CSCALE] * s0[S_BSCALE];
+    s.obj_const = s0[S_OBJC];
+    s.bnorm = s0[S_BNORM];
+    s.cnorm = s0[S_CNORM];
+    s.w = s0[S_W0];
     s.infeas_tol = infeas_tol;
     s.time_limit_s = time_limit;
     s.max_iter = max_iter;
@@ -559,64 +632,81 @@ __global__ void k_init_state(SolveState* st, const double* sc, double obj_const,
     s.has_q = has_q;
     s.carry_restart_err = -1.0;
     s.restart_err = -1.0;
-    *st = s;
+    s.t0_ns = global_ns();
+    st[k] = s;
+}
+
+__global__ void k_activate_all(int count, SolveState* st) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) st[k].active = st[k].in_phase = 1;
 }
 
 void sync_state(Problem& P) {
-    GB_CUDA(cudaMemcpyAsync(P.st_host, P.st.get(), sizeof(SolveState), cudaMemcpyDeviceToHost, P.stream));
+    GB_CUDA(cudaMemcpyAsync(P.st_host, P.st.get(), sizeof(SolveState) * P.count, cudaMemcpyDeviceToHost, P.stream));
     GB_CUDA(cudaStreamSynchronize(P.stream));
 }
 
 template <class M, class V>
-int run_phase(Problem& P, const gb_options* opt, double tol, int stall_exit, int stall_checks, bool first,
-              bool has_r) {
+void run_phase(Problem& P, const gb_options* opt, double tol, int stall_exit, int stall_checks, bool first,
+               bool has_r) {
     cudaStream_t s = P.stream;
     VecSet<V>& vs = Level<M, V>::vs(P);
     const int gv = elem_grid(std::max(P.n, P.m), P.sms);
-    k_phase_in<V><<<gv, kThreads, 0, s>>>(P.n, P.m, P.x64.get(), P.y64.get(), has_r ? P.xr64.get() : P.x64.get(),
-                                         has_r ? P.yr64.get() : P.y64.get(), vs.x0.get(), vs.y0.get(), vs.xr.get(),
-                                         vs.yr.get(), vs.sumx.get(), vs.sumy.get());
-    k_set_phase<<<1, 1, 0, s>>>(P.st.get(), tol, stall_checks, stall_exit, first ? 1 : 0);
+    long long checks_before = 0;
+    if (!first)
+        for (int k = 0; k < P.count; ++k) checks_before = std::max<long long>(checks_before, P.st_host[k].checks);
+    GB_CUDA(cudaMemcpyAsync(P.phase_flags.get(), P.phase_flags_host, sizeof(int) * P.count, cudaMemcpyHostToDevice,
+                            s));
+    k_set_phase<<<div_up(P.count, kThreads), kThreads, 0, s>>>(P.count, P.st.get(), P.phase_flags.get(), tol,
+                                                               stall_checks, stall_exit, first ? 1 : 0);
+    k_phase_in<V><<<gv, kThreads, 0, s>>>(P.n, P.m, P.icol(), P.irow(), P.st.get(), P.x64.get(), P.y64.get(),
+                                         P.xr64.get(), P.yr64.get(), has_r ? 1 : 0, vs.x0.get(), vs.y0.get(),
+                                         vs.xr.get(), vs.yr.get(), vs.sumx.get(), vs.sumy.get());
     P.launches += 2;
     if (P.has_q) launch_qx<M, V>(P, vs, vs.x0.get(), vs.qx.get(), s, P.launches);
     EvalArgs<M, V> ea = eval_args<M, V>(P, vs, vs.x0.get(), vs.y0.get(), kEvalInit, P.has_q);
     k_eval<M, V, 1, 1><<<P.A.sched.nb + P.AT.sched.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(ea);
     P.launches += 1;
-    const int checks_before = first ? 0 : P.st_host->checks;
     long long per_body = 0;
+    long long bodies = 0;
     if (host_loop_mode()) {
         // Same kernels, launched from a host loop with one state read-back per
         // check (profilers cannot see kernels inside conditional graphs).
         for (;;) {
             per_body = capture_body<M, V>(P, opt->check_every, 0, s, 0);
+            ++bodies;
             sync_state(P);
-            if (P.st_host->done) break;
+            bool any = false;
+            for (int k = 0; k < P.count; ++k) any |= P.st_host[k].active != 0;
+            if (!any) break;
         }
     } else {
         LevelGraph* g = level_graph<M, V>(P, opt->check_every);
         GB_CUDA(cudaGraphLaunch(g->exec, s));
         per_body = g->launches_per_body;
     }
-    k_phase_out<V><<<gv, kThreads, 0, s>>>(P.n, P.m, vs.x0.get(), vs.y0.get(), vs.sumx.get(), vs.sumy.get(),
-                                          vs.xr.get(), vs.yr.get(), P.st.get(), P.x64.get(), P.y64.get(),
-                                          P.xr64.get(), P.yr64.get());
+    k_phase_out<V><<<gv, kThreads, 0, s>>>(P.n, P.m, P.icol(), P.irow(), vs.x0.get(), vs.y0.get(), vs.sumx.get(),
+                                          vs.sumy.get(), vs.xr.get(), vs.yr.get(), P.st.get(), P.x64.get(),
+                                          P.y64.get(), P.xr64.get(), P.yr64.get());
     sync_state(P);
-    P.launches += 1 + static_cast<long long>(P.st_host->checks - checks_before) * per_body;
+    if (!host_loop_mode()) {
+        long long checks_after = 0;
+        for (int k = 0; k < P.count; ++k) checks_after = std::max<long long>(checks_after, P.st_host[k].checks);
+        bodies = checks_after - checks_before;
+    }
+    P.launches += 1 + bodies * per_body;
     GB_CUDA(cudaGetLastError());
-    return P.st_host->exit_reason;
 }
 
-// pdhg_evaluate<Bd> (pdhg_impl.hpp:202-230) of the carried FP64 state.
-Kkt certify(Problem& P) {
+// pdhg_evaluate<Bd> (pdhg_impl.hpp:202-230) of the carried FP64 state of every instance.
+void certify(Problem& P) {
     cudaStream_t s = P.stream;
     VecSet<double>& vs = P.v64;
     if (P.has_q) launch_qx<double, double>(P, vs, P.x64.get(), vs.qx.get(), s, P.launches);
     EvalArgs<double, double> ea = eval_args<double, double>(P, vs, P.x64.get(), P.y64.get(), kEvalCertify, P.has_q);
-    k_eval<double, double, 1, 1><<<P.A.sched.nb + P.AT.sched.nb, kThreads,
-                                   spmv_smem_bytes<1, double>(), s>>>(ea);
+    k_eval<double, double, 1, 1><<<P.A.sched.nb + P.AT.sched.nb, kThreads, spmv_smem_bytes<1, double>(), s>>>(ea);
     P.launches += 1;
     sync_state(P);
-    return P.st_host->kcert;
 }
 
 inline bool kkt_conv_h(const Kkt& k, double tol) { return k.rel_p <= tol && k.rel_d <= tol && k.rel_gap <= tol; }
@@ -631,76 +721,102 @@ int status_from(int e) {  // pdhg_impl.hpp:232-240
     }
 }
 
-// run_pdhg (pdhg_impl.hpp:243-328) with device-resident state.
+// run_pdhg (pdhg_impl.hpp:243-328) of every instance with device-resident state.
 void solve_problem(Problem& P, const gb_options* opt, gb_result* res) {
     GB_REQUIRE(opt->check_every > 0, "check_every must be positive");
     GB_REQUIRE(opt->precision >= 0 && opt->precision <= 2, "unknown precision");
     GB_CUDA(cudaSetDevice(P.device));
     cudaStream_t s = P.stream;
     const auto t0 = std::chrono::steady_clock::now();
+    const int K = P.count;
     P.launches = 0;
-    k_init_state<<<1, 1, 0, s>>>(P.st.get(), P.scal.get(), P.maximize ? -P.obj_const : P.obj_const,
-                                 P.has_q ? 1 : 0, opt->check_every, opt->max_iter, opt->time_limit, opt->infeas_tol);
+    k_init_state<<<div_up(K, kThreads), kThreads, 0, s>>>(K, P.st.get(), P.scal.get(), P.has_q ? 1 : 0,
+                                                          opt->check_every, opt->max_iter, opt->time_limit,
+                                                          opt->infeas_tol);
     k_start_point<<<elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s>>>(P.n, P.m, P.l.get(), P.u.get(),
                                                                          P.x64.get(), P.y64.get());
-    k_mark_start<<<1, 1, 0, s>>>(P.st.get());
-    P.launches += 3;
-    int ex;
-    long long fp32_iters = 0, l2_iters = 0;
-    int phases = 0;
-    auto finished = [&](int e) {
-        const Kkt k64 = certify(P);
-        return (e == kConverged && kkt_conv_h(k64, opt->tol)) || e == kTimeLimit || e == kIterLimit ||
-               e == kInfeasible;
+    P.launches += 2;
+    P.results.assign(K, InstanceResult{});
+    std::vector<int> ex(K, kIterLimit), done(K, 0);
+    auto set_flags = [&](auto pred) {
+        int any = 0;
+        for (int k = 0; k < K; ++k) any |= (P.phase_flags_host[k] = pred(k) ? 1 : 0);
+        return any != 0;
+    };
+    auto collect = [&]() {
+        for (int k = 0; k < K; ++k)
+            if (P.phase_flags_host[k]) {
+                ex[k] = P.st_host[k].exit_reason;
+                P.results[k].phases += 1;
+            }
+    };
+    // finished lambda (pdhg_impl.hpp:278-286) after the FP64 certification
+    auto finished = [&]() {
+        certify(P);
+        for (int k = 0; k < K; ++k) {
+            if (!P.phase_flags_host[k] || done[k]) continue;
+            const int e = ex[k];
+            done[k] = (e == kConverged && kkt_conv_h(P.st_host[k].kcert, opt->tol)) || e == kTimeLimit ||
+                      e == kIterLimit || e == kInfeasible;
+        }
     };
     if (opt->precision != GB_PREC_DOUBLE) {
-        ex = run_phase<float, float>(P, opt, opt->tol, 1, opt->stall_checks, true, false);
-        ++phases;
-        fp32_iters = P.st_host->it;
-        bool done = finished(ex);
-        if (!done && opt->precision == GB_PREC_DYNAMIC) {
-            ex = run_phase<float, double>(P, opt, opt->tol, 1, opt->stall_checks_l2, false, true);
-            ++phases;
-            l2_iters = P.st_host->it - fp32_iters;
-            done = finished(ex);
+        set_flags([](int) { return true; });
+        run_phase<float, float>(P, opt, opt->tol, 1, opt->stall_checks, true, false);
+        collect();
+        for (int k = 0; k < K; ++k) P.results[k].fp32_iters = P.st_host[k].it;
+        finished();
+        if (opt->precision == GB_PREC_DYNAMIC && set_flags([&](int k) { return !done[k]; })) {
+            run_phase<float, double>(P, opt, opt->tol, 1, opt->stall_checks_l2, false, true);
+            collect();
+            for (int k = 0; k < K; ++k)
+                if (P.phase_flags_host[k]) P.results[k].l2_iters = P.st_host[k].it - P.results[k].fp32_iters;
+            finished();
         }
-        if (!done) {
-            ex = run_phase<double, double>(P, opt, opt->tol, 0, 0, false, true);
-            ++phases;
+        if (set_flags([&](int k) { return !done[k]; })) {
+            run_phase<double, double>(P, opt, opt->tol, 0, 0, false, true);
+            collect();
         }
     } else {
-        ex = run_phase<double, double>(P, opt, opt->tol, 0, 0, true, false);
-        ++phases;
+        set_flags([](int) { return true; });
+        run_phase<double, double>(P, opt, opt->tol, 0, 0, true, false);
+        collect();
     }
-    const Kkt fin = certify(P);
-    int status = status_from(ex);
-    if (status == GB_OPTIMAL && !kkt_conv_h(fin, opt->tol * 1.0000001)) status = GB_NUMERICAL_ERROR;
-    const double sign = P.maximize ? -1.0 : 1.0;
-    k_unscale<<<elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s>>>(P.n, P.m, sign, P.x64.get(), P.y64.get(),
-                                                                     P.C.get(), P.R.get(), P.scal.get(),
-                                                                     P.xo.get(), P.yo.get());
+    // Final FP64 certification of the returned points.
+    certify(P);
+    k_unscale<<<elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s>>>(P.n, P.m, P.icol(), P.irow(), P.x64.get(),
+                                                                     P.y64.get(), P.C.get(), P.R.get(),
+                                                                     P.scal.get(), P.xo.get(), P.yo.get());
     P.launches += 1;
     GB_CUDA(cudaStreamSynchronize(s));
     GB_CUDA(cudaGetLastError());
-    const SolveState& st = *P.st_host;
-    if (res) {
-        std::memset(res, 0, sizeof(*res));
-        res->status = status;
-        res->pobj = sign * fin.pobj;
-        res->dobj = sign * fin.dobj;
-        res->rel_primal = fin.rel_p;
-        res->rel_dual = fin.rel_d;
-        res->rel_gap = fin.rel_gap;
-        res->iterations = st.it;
-        res->fp32_iterations = fp32_iters;
-        res->l2_iterations = l2_iters;
-        res->restarts = st.restarts;
-        res->setup_seconds = P.setup_seconds;
-        res->solve_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        res->norm_a = P.scal_host[2];
-        res->primal_weight = st.w;
-        res->checks = st.checks;
-        res->phases = phases;
+    const double solve_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    for (int k = 0; k < K; ++k) {
+        const SolveState& st = P.st_host[k];
+        const Kkt& fin = st.kcert;
+        int status = status_from(ex[k]);
+        if (status == GB_OPTIMAL && !kkt_conv_h(fin, opt->tol * 1.0000001)) status = GB_NUMERICAL_ERROR;
+        P.results[k].status = status;
+        if (!res) continue;
+        gb_result& r = res[k];
+        const double sign = P.maximize[k] ? -1.0 : 1.0;
+        std::memset(&r, 0, sizeof(r));
+        r.status = status;
+        r.pobj = sign * fin.pobj;
+        r.dobj = sign * fin.dobj;
+        r.rel_primal = fin.rel_p;
+        r.rel_dual = fin.rel_d;
+        r.rel_gap = fin.rel_gap;
+        r.iterations = st.it;
+        r.fp32_iterations = P.results[k].fp32_iters;
+        r.l2_iterations = P.results[k].l2_iters;
+        r.restarts = st.restarts;
+        r.setup_seconds = P.setup_seconds;
+        r.solve_seconds = solve_s;
+        r.norm_a = P.scal_host[static_cast<size_t>(k) * kScal + S_NORMA];
+        r.primal_weight = st.w;
+        r.checks = st.checks;
+        r.phases = P.results[k].phases;
     }
     P.solved = true;
 }
@@ -710,32 +826,18 @@ template <class M, class V>
 void time_level(Problem& P, int iters, double* msp, double* msd, int64_t* launches) {
     cudaStream_t s = P.stream;
     VecSet<V>& vs = Level<M, V>::vs(P);
-    // a valid iterate: the start point with current step sizes
+    k_activate_all<<<div_up(P.count, kThreads), kThreads, 0, s>>>(P.count, P.st.get());
     k_phase_in<V><<<elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s>>>(
-        P.n, P.m, P.x64.get(), P.y64.get(), P.x64.get(), P.y64.get(), vs.x0.get(), vs.y0.get(), vs.xr.get(),
-        vs.yr.get(), vs.sumx.get(), vs.sumy.get());
+        P.n, P.m, P.icol(), P.irow(), P.st.get(), P.x64.get(), P.y64.get(), P.x64.get(), P.y64.get(), 0,
+        vs.x0.get(), vs.y0.get(), vs.xr.get(), vs.yr.get(), vs.sumx.get(), vs.sumy.get());
     std::vector<cudaEvent_t> ev(2 * iters + 1);
     for (auto& e : ev) GB_CUDA(cudaEventCreate(&e));
     long long nl = 0;
-    // warm-up
-    for (int k = 0; k < 4; ++k) launch_iteration<M, V>(P, vs, k, s, nl);
+    for (int k = 0; k < 4; ++k) launch_iteration<M, V>(P, vs, k, s, nl);  // warm-up
     GB_CUDA(cudaEventRecord(ev[0], s));
     for (int k = 0; k < iters; ++k) {
-        const V* xin = (k & 1) ? vs.x1.get() : vs.x0.get();
-        V* xout = (k & 1) ? vs.x0.get() : vs.x1.get();
-        const V* yin = (k & 1) ? vs.y1.get() : vs.y0.get();
-        V* yout = (k & 1) ? vs.y0.get() : vs.y1.get();
-        if (P.has_q) launch_qx<M, V>(P, vs, xin, vs.qx.get(), s, nl);
-        constexpr size_t sm = spmv_smem_bytes<1, V>();
-        PrimalArgs<M, V> pa{P.AT.view<M>(), yin, xin, vs.c.get(), vs.l.get(), vs.u.get(),
-                            P.has_q ? vs.qx.get() : nullptr, xout, vs.xbar.get(), vs.sumx.get(), P.st.get()};
-        k_primal<M, V><<<P.AT.sched.nb, kThreads, sm, s>>>(pa);
-        GB_CUDA(cudaEventRecord(ev[2 * k + 1], s));
-        DualArgs<M, V> da{P.A.view<M>(), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(),
-                          P.st.get()};
-        k_dual<M, V><<<P.A.sched.nb, kThreads, sm, s>>>(da);
+        launch_iteration<M, V>(P, vs, k, s, nl, ev[2 * k + 1]);
         GB_CUDA(cudaEventRecord(ev[2 * k + 2], s));
-        nl += 2;
     }
     GB_CUDA(cudaStreamSynchronize(s));
     double tp = 0, td = 0;
@@ -752,12 +854,32 @@ void time_level(Problem& P, int iters, double* msp, double* msd, int64_t* launch
     *launches = nl;
 }
 
+void problem_stats(const Problem& P, int64_t* launches, double* bpi) {
+    if (launches) *launches = P.launches;
+    if (bpi) {
+        // fused iteration: 2 nnz (s_M + 4) + 4 (m + n + 2) + s_V (9 n + 7 m)  (+ Q for QP)
+        const double nnz = static_cast<double>(P.A.nnz), n = P.n, m = P.m;
+        const double sm[3] = {4, 4, 8}, sv[3] = {4, 8, 8};
+        for (int l = 0; l < 3; ++l) {
+            double b = 2 * nnz * (sm[l] + 4) + 4 * (m + n + 2) + sv[l] * (9 * n + 7 * m);
+            if (P.has_q) {
+                if (P.dplr) b += 2.0 * n * P.qk * sv[l] + 2 * n * sv[l];
+                else b += static_cast<double>(P.Q.nnz) * (sm[l] + 4) + 4 * (n + 1) + sv[l] * 2 * n;
+            }
+            bpi[l] = b;
+        }
+    }
+}
+
 }  // namespace gb
 
 // ==================================================================== C ABI
 using namespace gb;
 
 struct gb_problem {
+    Problem* p;
+};
+struct gb_batch {
     Problem* p;
 };
 
@@ -794,7 +916,7 @@ int gb_problem_create(const gb_lp* lp, const gb_options* opt, gb_problem** out) 
         GB_REQUIRE(out != nullptr, "out is NULL");
         gb_options def;
         gb_default_options(&def);
-        Problem* p = create_problem(lp, opt ? opt : &def);
+        Problem* p = create_problem(1, lp, opt ? opt : &def);
         *out = new gb_problem{p};
     });
 }
@@ -841,21 +963,7 @@ int gb_problem_time_kernels(gb_problem* p, int level, int iters, double* ms_prim
 int gb_problem_stats(gb_problem* p, int64_t* launches, double* bpi) {
     return guarded([&] {
         GB_REQUIRE(p != nullptr, "problem is NULL");
-        Problem& P = *p->p;
-        if (launches) *launches = P.launches;
-        if (bpi) {
-            // fused iteration: 2 nnz (s_M + 4) + 4 (m + n + 2) + s_V (9 n + 7 m)  (+ Q for QP)
-            const double nnz = static_cast<double>(P.A.nnz), n = P.n, m = P.m;
-            const double sm[3] = {4, 4, 8}, sv[3] = {4, 8, 8};
-            for (int l = 0; l < 3; ++l) {
-                double b = 2 * nnz * (sm[l] + 4) + 4 * (m + n + 2) + sv[l] * (9 * n + 7 * m);
-                if (P.has_q) {
-                    if (P.dplr) b += 2.0 * n * P.qk * sv[l] + 2 * n * sv[l];
-                    else b += static_cast<double>(P.Q.nnz) * (sm[l] + 4) + 4 * (n + 1) + sv[l] * 2 * n;
-                }
-                bpi[l] = b;
-            }
-        }
+        problem_stats(*p->p, launches, bpi);
     });
 }
 
@@ -864,12 +972,85 @@ int gb_solve(const gb_lp* lp, const gb_options* opt, gb_result* res, double* x_o
         gb_options def;
         gb_default_options(&def);
         const gb_options* o = opt ? opt : &def;
-        std::unique_ptr<Problem> P(create_problem(lp, o));
+        std::unique_ptr<Problem> P(create_problem(1, lp, o));
         solve_problem(*P, o, res);
         if (x_out) P->xo.download(x_out, P->n, P->stream);
         if (y_out) P->yo.download(y_out, P->m, P->stream);
         GB_CUDA(cudaStreamSynchronize(P->stream));
     });
+}
+
+// ---- batched solving (one block-diagonal resident problem)
+int gb_batch_create(int count, const gb_lp* lps, const gb_options* opt, gb_batch** out) {
+    return guarded([&] {
+        GB_REQUIRE(out != nullptr && count >= 1, "bad arguments");
+        gb_options def;
+        gb_default_options(&def);
+        Problem* p = create_problem(count, lps, opt ? opt : &def);
+        *out = new gb_batch{p};
+    });
+}
+
+int gb_batch_solve(gb_batch* b, const gb_options* opt, gb_result* results) {
+    return guarded([&] {
+        GB_REQUIRE(b != nullptr, "batch is NULL");
+        gb_options def;
+        gb_default_options(&def);
+        solve_problem(*b->p, opt ? opt : &def, results);
+    });
+}
+
+int gb_batch_get_solution(gb_batch* b, int i, double* x_out, double* y_out) {
+    return guarded([&] {
+        GB_REQUIRE(b != nullptr && b->p->solved, "no solution available");
+        Problem& P = *b->p;
+        GB_REQUIRE(i >= 0 && i < P.count, "instance index out of range");
+        const int c0 = P.col_off[i], c1 = P.col_off[i + 1], r0 = P.row_off[i], r1 = P.row_off[i + 1];
+        if (x_out && c1 > c0)
+            GB_CUDA(cudaMemcpyAsync(x_out, P.xo.get() + c0, sizeof(double) * (c1 - c0), cudaMemcpyDeviceToHost,
+                                    P.stream));
+        if (y_out && r1 > r0)
+            GB_CUDA(cudaMemcpyAsync(y_out, P.yo.get() + r0, sizeof(double) * (r1 - r0), cudaMemcpyDeviceToHost,
+                                    P.stream));
+        GB_CUDA(cudaStreamSynchronize(P.stream));
+    });
+}
+
+int gb_batch_schedule(gb_batch* b, int* threads, int* blocks_per_sm, int* groups) {
+    return guarded([&] {
+        GB_REQUIRE(b != nullptr, "batch is NULL");
+        Problem& P = *b->p;
+        if (threads) *threads = kThreads;
+        if (blocks_per_sm) {
+            int o = 0;
+            GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_dual<float, float>, kThreads,
+                                                                  spmv_smem_bytes<1, float>()));
+            *blocks_per_sm = o;
+        }
+        if (groups) {
+            // group size (lanes per row) used by most of an instance's STREAM-block nonzeros
+            std::vector<RowBlock> ba(P.A.sched.nb), bt(P.AT.sched.nb);
+            P.A.sched.blocks.download(ba.data(), ba.size(), P.stream);
+            P.AT.sched.blocks.download(bt.data(), bt.size(), P.stream);
+            GB_CUDA(cudaStreamSynchronize(P.stream));
+            auto mode_g = [](const std::vector<RowBlock>& bl, int b0, int b1) {
+                int cnt[6] = {0};
+                for (int i = b0; i < b1; ++i)
+                    if (bl[i].kind == kStream) cnt[std::min(bl[i].lg, 5)] += bl[i].p1 - bl[i].p0;
+                return 1 << static_cast<int>(std::max_element(cnt, cnt + 6) - cnt);
+            };
+            for (int k = 0; k < P.count; ++k) {
+                groups[2 * k] = mode_g(ba, P.A.sched.host_seg_block[k], P.A.sched.host_seg_block[k + 1]);
+                groups[2 * k + 1] = mode_g(bt, P.AT.sched.host_seg_block[k], P.AT.sched.host_seg_block[k + 1]);
+            }
+        }
+    });
+}
+
+void gb_batch_destroy(gb_batch* b) {
+    if (!b) return;
+    delete b->p;
+    delete b;
 }
 
 }  // extern "C"

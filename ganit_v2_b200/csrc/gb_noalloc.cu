@@ -33,7 +33,8 @@ constexpr size_t kOffBlocks = 512;
 constexpr size_t kOffPartials = kOffBlocks + sizeof(RowBlock) * GB_NOALLOC_MAX_BLOCKS;
 constexpr size_t kOffSlots = kOffPartials + sizeof(double) * kTerms * GB_NOALLOC_MAX_BLOCKS;
 constexpr size_t kOffCounters = kOffSlots + sizeof(double) * GB_NOALLOC_MAX_SLOTS;
-constexpr size_t kOffEnd = kOffCounters + sizeof(unsigned) * GB_NOALLOC_MAX_LONG_ROWS;
+constexpr size_t kOffSeg = kOffCounters + sizeof(unsigned) * GB_NOALLOC_MAX_LONG_ROWS;  // 2 x int[2] + arrive
+constexpr size_t kOffEnd = kOffSeg + 64;
 static_assert(sizeof(SolveState) <= kOffBlocks, "state slot too small");
 static_assert(kOffEnd <= kNoAllocScratchBytes, "scratch layout exceeds the array");
 
@@ -83,11 +84,11 @@ extern "C" int gb_eval_kkt_noalloc(const gb_scaled_lp* dev, const int32_t* h_a_p
             if (nb >= GB_NOALLOC_MAX_BLOCKS) { overflow = true; return; }
             g_noalloc_blocks[nb++] = b;
         };
-        schedule_rows(h_a_ptr, dev->m, kBlockNnz, kThreads, &nslots, &ncounters, emit);
+        schedule_rows(h_a_ptr, 0, dev->m, kBlockNnz, kThreads, &nslots, &ncounters, 0, emit);
         const int nbA = nb;
         const int slotsA = nslots, countersA = ncounters;
         int nslotsT = 0, ncountersT = 0;
-        schedule_rows(h_at_ptr, dev->n, kBlockNnz, kThreads, &nslotsT, &ncountersT, emit);
+        schedule_rows(h_at_ptr, 0, dev->n, kBlockNnz, kThreads, &nslotsT, &ncountersT, 0, emit);
         if (overflow || nslots + nslotsT > GB_NOALLOC_MAX_SLOTS || ncounters + ncountersT > GB_NOALLOC_MAX_LONG_ROWS)
             throw Error(GB_ERR_INVALID,
                         "problem too large for gb_eval_kkt_noalloc: needs " + std::to_string(nb) + "+ row blocks, " +
@@ -101,15 +102,20 @@ extern "C" int gb_eval_kkt_noalloc(const gb_scaled_lp* dev, const int32_t* h_a_p
         double* partials = reinterpret_cast<double*>(base + kOffPartials);
         double* slots = reinterpret_cast<double*>(base + kOffSlots);
         unsigned* counters = reinterpret_cast<unsigned*>(base + kOffCounters);
+        int* seg = reinterpret_cast<int*>(base + kOffSeg);  // A blocks [0, nbA), A^T blocks [0, nb - nbA)
+        unsigned* arrive = reinterpret_cast<unsigned*>(base + kOffSeg + 32);
+        const int hseg[4] = {0, nbA, 0, nb - nbA};
+        static_assert(sizeof(hseg) <= 32, "segment slot");
         GB_CUDA(cudaMemcpyAsync(blocks, g_noalloc_blocks, sizeof(RowBlock) * nb, cudaMemcpyHostToDevice, s));
         GB_CUDA(cudaMemsetAsync(counters, 0, sizeof(unsigned) * GB_NOALLOC_MAX_LONG_ROWS, s));
+        GB_CUDA(cudaMemcpyAsync(seg, hseg, sizeof(hseg), cudaMemcpyHostToDevice, s));
+        GB_CUDA(cudaMemsetAsync(arrive, 0, sizeof(unsigned), s));
         SolveState h;
         std::memset(&h, 0, sizeof(h));
         h.obj_scale = sc->obj_scale;
         h.obj_const = sc->obj_const;
         h.bnorm = sc->bnorm;
         h.cnorm = sc->cnorm;
-        h.arrive = 0u;
         GB_CUDA(cudaMemcpyAsync(st, &h, sizeof(h), cudaMemcpyHostToDevice, s));
 
         EvalArgs<double, double> a;
@@ -122,6 +128,10 @@ extern "C" int gb_eval_kkt_noalloc(const gb_scaled_lp* dev, const int32_t* h_a_p
         a.x = x; a.y = y;
         a.c = dev->c; a.l = dev->l; a.u = dev->u; a.lo = dev->lo; a.hi = dev->hi; a.rres = dev->rres; a.cres = dev->cres;
         a.mode = kEvalCertify;
+        a.count = 1;
+        a.seg_a = seg;
+        a.seg_t = seg + 2;
+        a.arrive = arrive;
         a.st = st;
         a.partials = partials;
         a.use_cond = 0;

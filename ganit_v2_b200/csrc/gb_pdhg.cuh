@@ -1,4 +1,11 @@
-// Fused restarted-PDHG kernels for one problem instance.
+// Fused restarted-PDHG kernels over a batch of instances (one instance = the
+// single-problem case).
+//
+// A batch is one block-diagonal problem: instance k owns rows
+// [row_off[k], row_off[k+1]) of A and columns [col_off[k], col_off[k+1]); every
+// row block of the schedules belongs to exactly one instance, so a block reads
+// its instance's step sizes and is skipped once that instance has stopped
+// iterating.
 //
 // Per iteration (src/pdhg_impl.hpp:133-139) two launches:
 //   k_primal : rows j of the stored transpose: aty_j = (A^T y)_j, then the
@@ -9,11 +16,12 @@
 // Every check_every iterations (pdhg_impl.hpp:142-190) one k_eval launch
 // computes, for the current iterate, the running average and the ray y - y_r,
 // all KKT pieces of pdhg_impl.hpp:92-118 in FP64 (one pass over A and one
-// over A^T, several right-hand sides per pass), and its last CTA reduces the
-// per-CTA partials in a fixed order and runs the whole scalar decision of
-// pdhg_impl.hpp:144-189 (convergence, limits, infeasibility certificate,
-// stall exit, adaptive restart, primal-weight update).  k_restart applies a
-// restart.  No host round trip happens inside a precision phase.
+// over A^T, several right-hand sides per pass); its last CTA reduces each
+// instance's per-CTA partials in a fixed order and runs, one thread per
+// instance, the whole scalar decision of pdhg_impl.hpp:144-189 (convergence,
+// limits, infeasibility certificate, stall exit, adaptive restart, primal
+// weight).  k_restart applies restarts.  No host round trip happens inside a
+// precision phase.
 #pragma once
 #include "gb_spmv.cuh"
 
@@ -27,8 +35,8 @@ struct Kkt {
 enum PhaseExit : int { kConverged = 0, kStalled = 1, kIterLimit = 2, kTimeLimit = 3, kInfeasible = 4, kNumerical = 5 };
 enum EvalMode : int { kEvalInit = 0, kEvalCheck = 1, kEvalCertify = 2 };
 
-// Device-resident solver state (PdhgShared + PdhgState + loop locals of
-// pdhg_impl.hpp:44-63, 120-128).  Scalars are FP64.
+// Device-resident solver state of one instance (PdhgShared + PdhgState + loop
+// locals of pdhg_impl.hpp:44-63, 120-128).  Scalars are FP64.
 struct alignas(16) SolveState {
     // problem constants
     double eta, normA, normQ, obj_scale, obj_const, bnorm, cnorm;
@@ -51,7 +59,10 @@ struct alignas(16) SolveState {
     int restart_now, avg_better, done, exit_reason, best_is_avg;
     double inv_avg;
     Kkt best, kcert, kc, ka;
-    unsigned arrive;           // CTA arrival counter of k_eval (re-armed by the last CTA)
+    int active;                // iterating in the current phase
+    int in_phase;              // took part in the current phase
+    int ran_body;              // iterated during the body that ended at the last check
+    int pad_;
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -64,6 +75,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // Minimum resident CTAs per SM requested from the register allocator.
 template <class V>
 constexpr int kMinCtas = sizeof(V) == 4 ? 8 : 6;
+
 template <class M, class V>
 struct PrimalArgs {
     CsrView<M> AT;
@@ -76,13 +88,18 @@ struct PrimalArgs {
     V* __restrict__ xn;
     V* __restrict__ xbar;
     V* __restrict__ sumx;
-    const SolveState* st;
+    const SolveState* st;       // per instance
 };
 
 template <class M, class V>
 struct PrimalEpi {
     const PrimalArgs<M, V>* a;  // kernel parameter space (__grid_constant__)
     V tau;
+    __device__ __forceinline__ bool begin(int inst) {
+        const SolveState& s = a->st[inst];
+        tau = static_cast<V>(s.tau);
+        return s.active != 0;
+    }
     struct Pre {
         V x, c, l, u, sumx, qx;
     };
@@ -103,7 +120,7 @@ struct PrimalEpi {
 template <class M, class V>
 __global__ void __launch_bounds__(kThreads, kMinCtas<V>) k_primal(const __grid_constant__ PrimalArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    PrimalEpi<M, V> epi{&a, static_cast<V>(a.st->tau)};
+    PrimalEpi<M, V> epi{&a, V(0)};
     spmv_run<1, M, V>(a.AT, blockIdx.x, GatherOne<V>{a.y}, epi, smem);
 }
 
@@ -116,13 +133,18 @@ struct DualArgs {
     const V* __restrict__ hi;
     V* __restrict__ yn;
     V* __restrict__ sumy;
-    const SolveState* st;
+    const SolveState* st;       // per instance
 };
 
 template <class M, class V>
 struct DualEpi {
     const DualArgs<M, V>* a;  // kernel parameter space (__grid_constant__)
     V sigma;
+    __device__ __forceinline__ bool begin(int inst) {
+        const SolveState& s = a->st[inst];
+        sigma = static_cast<V>(s.sigma);
+        return s.active != 0;
+    }
     struct Pre {
         V y, lo, hi, sumy;
     };
@@ -142,7 +164,7 @@ struct DualEpi {
 template <class M, class V>
 __global__ void __launch_bounds__(kThreads, kMinCtas<V>) k_dual(const __grid_constant__ DualArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    DualEpi<M, V> epi{&a, static_cast<V>(a.st->sigma)};
+    DualEpi<M, V> epi{&a, V(0)};
     spmv_run<1, M, V>(a.A, blockIdx.x, GatherOne<V>{a.xbar}, epi, smem);
 }
 
@@ -173,7 +195,11 @@ struct EvalArgs {
     const V* __restrict__ qx;    // Q x   (QP) or nullptr
     const V* __restrict__ qxa;   // Q xa  (QP, check mode) or nullptr
     int mode;
-    SolveState* st;
+    int count;                   // instances
+    const int* seg_a;            // instance k owns A blocks [seg_a[k], seg_a[k+1])
+    const int* seg_t;            // and A^T blocks [seg_t[k], seg_t[k+1])
+    SolveState* st;              // per instance
+    unsigned* arrive;            // CTA arrival counter (re-armed by the last CTA)
     double* partials;            // [gridDim.x][kTerms]
     unsigned long long cond;     // cudaGraphConditionalHandle of the phase loop
     int use_cond;                // 1 inside the loop body: the decision drives the loop
@@ -211,12 +237,23 @@ struct GatherYAvgRay {  // A^T side: y, ya and the ray y - yr
     }
 };
 
+// 1 / it_since at the coming check of an instance (the average's weight).
+__device__ __forceinline__ double avg_weight(const SolveState& s, int mode) {
+    return mode == kEvalCheck ? 1.0 / static_cast<double>(s.it_since + s.check_every) : 0.0;
+}
+
+// Evaluated instances: every instance when certifying, else the iterating ones.
+__device__ __forceinline__ bool eval_includes(const SolveState& s, int mode) {
+    return mode == kEvalCertify || s.active != 0;
+}
+
 // Per-row terms (backend_cpu.cpp:101-112, 132-142) and restart distances.
 template <class M, class V, int NV>
 struct EvalRowEpi {
     const EvalArgs<M, V>& a;  // kernel parameter space (__grid_constant__)
     double inv;
     double t[kTerms];
+    __device__ __forceinline__ bool begin(int inst) { return eval_includes(a.st[inst], a.mode); }
     __device__ __forceinline__ static double pres2(double ax, double lo, double hi, double r) {
         double p = (ax < lo) ? lo : ax;
         p = (hi < p) ? hi : p;
@@ -254,6 +291,7 @@ struct EvalColEpi {
     const EvalArgs<M, V>& a;  // kernel parameter space (__grid_constant__)
     double inv;
     double t[kTerms];
+    __device__ __forceinline__ bool begin(int inst) { return eval_includes(a.st[inst], a.mode); }
     __device__ __forceinline__ static void dres(double z, double lj, double uj, double cres, double& rd2,
                                                 double& ob) {
         double r = 0.0;
@@ -313,7 +351,7 @@ __device__ __forceinline__ void step_sizes(SolveState& s) {  // pdhg_impl.hpp:87
     }
 }
 
-// Scalar decision logic, run by one thread after all partials are reduced.
+// Scalar decision logic of one instance, after its partials are reduced.
 static __device__ void decide(SolveState& s, const double (&T)[kTerms], int mode) {
     const Kkt kc = make_kkt(s, T[T_CX_C], T[T_XQX_C], T[T_ROBJ_C], T[T_VOBJ_C], T[T_RP2_C], T[T_RD2_C]);
     if (mode == kEvalCertify) { s.kcert = kc; return; }
@@ -389,6 +427,8 @@ static __device__ void decide(SolveState& s, const double (&T)[kTerms], int mode
             s.restarts += 1;
         }
         step_sizes(s);
+    } else {
+        s.active = 0;  // this instance leaves the phase
     }
 }
 
@@ -397,12 +437,10 @@ __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalA
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double red[kWarps * kTerms];
     __shared__ bool am_last;
-    const int nctaA = a.A.nb;
-    const double inv = (a.mode == kEvalCheck)
-                           ? 1.0 / static_cast<double>(a.st->it_since + a.st->check_every)
-                           : 0.0;
+    const int nbA = a.A.nb;
     double t[kTerms];
-    if (static_cast<int>(blockIdx.x) < nctaA) {
+    if (static_cast<int>(blockIdx.x) < nbA) {
+        const double inv = avg_weight(a.st[a.A.blocks[blockIdx.x].inst], a.mode);
         EvalRowEpi<M, V, NVA> epi{a, inv, {}};
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) epi.t[k] = 0.0;
@@ -410,10 +448,12 @@ __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalA
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) t[k] = epi.t[k];
     } else {
+        const int cta = blockIdx.x - nbA;
+        const double inv = avg_weight(a.st[a.AT.blocks[cta].inst], a.mode);
         EvalColEpi<M, V, NVT> epi{a, inv, {}};
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) epi.t[k] = 0.0;
-        spmv_run<NVT, M, V>(a.AT, blockIdx.x - nctaA, GatherYAvgRay<V, NVT>{a.y, a.sumy, a.yr, inv}, epi, smem);
+        spmv_run<NVT, M, V>(a.AT, cta, GatherYAvgRay<V, NVT>{a.y, a.sumy, a.yr, inv}, epi, smem);
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) t[k] = epi.t[k];
     }
@@ -422,65 +462,83 @@ __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalA
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) a.partials[static_cast<size_t>(blockIdx.x) * kTerms + k] = t[k];
         __threadfence();
-        const unsigned prev = atomicAdd(&a.st->arrive, 1u);
+        const unsigned prev = atomicAdd(a.arrive, 1u);
         am_last = (prev == gridDim.x - 1);
     }
     __syncthreads();
     if (!am_last) return;
-    // last CTA: fixed-order reduction of all partials, then the decision
+    // last CTA: each thread reduces whole instances (their blocks, in block
+    // order) and runs their decisions
     __threadfence();
-    double T[kTerms];
-#pragma unroll
-    for (int k = 0; k < kTerms; ++k) T[k] = 0.0;
-    for (int blk = threadIdx.x; blk < static_cast<int>(gridDim.x); blk += kThreads) {
-#pragma unroll
-        for (int k = 0; k < kTerms; ++k) T[k] += __ldcg(a.partials + static_cast<size_t>(blk) * kTerms + k);
-    }
-    block_sum<kTerms>(T, red);
-    if (threadIdx.x == 0) {
-        SolveState& s = *a.st;
-        s.arrive = 0u;
-        decide(s, T, a.mode);
-        if (a.use_cond) {
-            cudaGraphSetConditional(static_cast<cudaGraphConditionalHandle>(a.cond),
-                                    (a.mode == kEvalCheck && s.done) ? 0u : 1u);
+    int any_active = 0;
+    for (int k = threadIdx.x; k < a.count; k += kThreads) {
+        SolveState& s = a.st[k];
+        if (!eval_includes(s, a.mode)) {
+            s.ran_body = 0;
+            continue;
         }
+        double T[kTerms];
+#pragma unroll
+        for (int q = 0; q < kTerms; ++q) T[q] = 0.0;
+        for (int b = a.seg_a[k]; b < a.seg_a[k + 1]; ++b) {
+#pragma unroll
+            for (int q = 0; q < kTerms; ++q) T[q] += __ldcg(a.partials + static_cast<size_t>(b) * kTerms + q);
+        }
+        for (int b = a.seg_t[k]; b < a.seg_t[k + 1]; ++b) {
+#pragma unroll
+            for (int q = 0; q < kTerms; ++q)
+                T[q] += __ldcg(a.partials + static_cast<size_t>(nbA + b) * kTerms + q);
+        }
+        s.ran_body = (a.mode == kEvalCheck) ? 1 : 0;
+        decide(s, T, a.mode);
+        any_active |= s.active;
+    }
+    any_active = __syncthreads_or(any_active);
+    if (threadIdx.x == 0) {
+        *a.arrive = 0u;
+        if (a.use_cond) cudaGraphSetConditional(static_cast<cudaGraphConditionalHandle>(a.cond), any_active ? 1u : 0u);
     }
 }
 
 // Restart / buffer bookkeeping after a check (pdhg_impl.hpp:178-185).
-// `xc`/`yc` hold the current iterate (buffer 1 when check_every is odd);
-// the result always lands in buffer 0 (x0, y0).
+// `xc`/`yc` hold the current iterate (buffer 1 when check_every is odd); the
+// result always lands in buffer 0 (x0, y0).  Only instances that iterated in
+// the body just checked are touched.
 template <class V>
 struct RestartArgs {
     const V* xc; const V* yc;
     V* x0; V* y0; V* xr; V* yr; V* sumx; V* sumy;
     int n, m;
+    const int* inst_col;   // column -> instance (nullptr: one instance)
+    const int* inst_row;   // row -> instance
     const SolveState* st;
 };
 
 template <class V>
 __global__ void k_restart(const RestartArgs<V> a) {
-    const SolveState& s = *a.st;
-    const bool restart = s.restart_now != 0;
     const bool copy = a.xc != a.x0;
-    if (!restart && !copy) return;
-    const bool avg = s.avg_better != 0;
-    const double inv = s.inv_avg;
     const int stride = gridDim.x * blockDim.x;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < a.n; j += stride) {
+        const SolveState& s = a.st[a.inst_col ? a.inst_col[j] : 0];
+        if (!s.ran_body) continue;
+        const bool restart = s.restart_now != 0;
+        if (!restart && !copy) continue;
         V v = a.xc[j];
         if (restart) {
-            if (avg) v = avg_of(a.sumx, j, inv);
+            if (s.avg_better) v = avg_of(a.sumx, j, s.inv_avg);
             a.xr[j] = v;
             a.sumx[j] = V(0);
         }
         a.x0[j] = v;
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.m; i += stride) {
+        const SolveState& s = a.st[a.inst_row ? a.inst_row[i] : 0];
+        if (!s.ran_body) continue;
+        const bool restart = s.restart_now != 0;
+        if (!restart && !copy) continue;
         V v = a.yc[i];
         if (restart) {
-            if (avg) v = avg_of(a.sumy, i, inv);
+            if (s.avg_better) v = avg_of(a.sumy, i, s.inv_avg);
             a.yr[i] = v;
             a.sumy[i] = V(0);
         }
@@ -489,44 +547,45 @@ __global__ void k_restart(const RestartArgs<V> a) {
 }
 
 // Phase start: iterate, restart point and zero sums in precision V from the
-// FP64 carried state (pdhg_impl.hpp:78-84).
+// FP64 carried state (pdhg_impl.hpp:78-84), for the instances in the phase.
 template <class V>
-__global__ void k_phase_in(int n, int m, const double* x64, const double* y64, const double* xr64,
-                           const double* yr64, V* x, V* y, V* xr, V* yr, V* sumx, V* sumy) {
+__global__ void k_phase_in(int n, int m, const int* inst_col, const int* inst_row, const SolveState* st,
+                           const double* x64, const double* y64, const double* xr64, const double* yr64,
+                           int has_r, V* x, V* y, V* xr, V* yr, V* sumx, V* sumy) {
     const int stride = gridDim.x * blockDim.x;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        if (!st[inst_col ? inst_col[j] : 0].in_phase) continue;
         x[j] = static_cast<V>(x64[j]);
-        xr[j] = static_cast<V>(xr64[j]);
+        xr[j] = static_cast<V>(has_r ? xr64[j] : x64[j]);
         sumx[j] = V(0);
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        if (!st[inst_row ? inst_row[i] : 0].in_phase) continue;
         y[i] = static_cast<V>(y64[i]);
-        yr[i] = static_cast<V>(yr64[i]);
+        yr[i] = static_cast<V>(has_r ? yr64[i] : y64[i]);
         sumy[i] = V(0);
     }
 }
 
 // Phase end: best point (current or average) and restart point to FP64
-// (pdhg_impl.hpp:191-194).
+// (pdhg_impl.hpp:191-194), for the instances in the phase.
 template <class V>
-__global__ void k_phase_out(int n, int m, const V* x, const V* y, const V* sumx, const V* sumy, const V* xr,
-                            const V* yr, const SolveState* st, double* x64, double* y64, double* xr64,
-                            double* yr64) {
-    const bool avg = st->best_is_avg != 0;
-    const double inv = st->inv_avg;
+__global__ void k_phase_out(int n, int m, const int* inst_col, const int* inst_row, const V* x, const V* y,
+                            const V* sumx, const V* sumy, const V* xr, const V* yr, const SolveState* st,
+                            double* x64, double* y64, double* xr64, double* yr64) {
     const int stride = gridDim.x * blockDim.x;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
-        x64[j] = static_cast<double>(avg ? avg_of(sumx, j, inv) : x[j]);
+        const SolveState& s = st[inst_col ? inst_col[j] : 0];
+        if (!s.in_phase) continue;
+        x64[j] = static_cast<double>(s.best_is_avg ? avg_of(sumx, j, s.inv_avg) : x[j]);
         xr64[j] = static_cast<double>(xr[j]);
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
-        y64[i] = static_cast<double>(avg ? avg_of(sumy, i, inv) : y[i]);
+        const SolveState& s = st[inst_row ? inst_row[i] : 0];
+        if (!s.in_phase) continue;
+        y64[i] = static_cast<double>(s.best_is_avg ? avg_of(sumy, i, s.inv_avg) : y[i]);
         yr64[i] = static_cast<double>(yr[i]);
     }
-}
-
-static __global__ void k_mark_start(SolveState* st) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) st->t0_ns = global_ns();
 }
 
 }  // namespace gb

@@ -1,6 +1,7 @@
-// Host-side engine for one resident problem: upload, device setup, precision
-// phases driven by per-level CUDA graphs whose body (check_every iterations +
-// KKT check + restart) repeats inside a device-side while loop.
+// Host-side engine state for a resident batch of problems (one problem is a
+// batch of one): upload, device setup, precision phases driven by per-level
+// CUDA graphs whose body (check_every iterations + KKT check + restart)
+// repeats inside a device-side while loop.
 #pragma once
 #include <chrono>
 #include <memory>
@@ -46,7 +47,6 @@ struct VecSet {
     DevBuf<V> c, l, u, lo, hi, rres, cres;
     DevBuf<V> x0, x1, xbar, y0, y1, sumx, sumy, xr, yr, qx, qxa;
     DevBuf<V> F, D;  // DPLR factor (n x k) and diagonal in precision V
-    DevBuf<V> ftx;   // F^T x partials / results (QP)
     void alloc(int n, int m, int qk, bool has_q) {
         for (DevBuf<V>* b : {&c, &l, &u, &cres, &x0, &x1, &xbar, &sumx, &xr}) b->reset(n ? n : 1);
         for (DevBuf<V>* b : {&lo, &hi, &rres, &y0, &y1, &sumy, &yr}) b->reset(m ? m : 1);
@@ -57,7 +57,6 @@ struct VecSet {
         if (qk > 0) {
             F.reset(static_cast<size_t>(n) * qk);
             D.reset(n);
-            ftx.reset(static_cast<size_t>(2) * qk);
         }
     }
 };
@@ -73,36 +72,56 @@ struct LevelGraph {
     }
 };
 
+// Per-instance outcome of a solve.
+struct InstanceResult {
+    int status = GB_NUMERICAL_ERROR;
+    long long fp32_iters = 0, l2_iters = 0;
+    int phases = 0;
+};
+
 struct Problem {
     int device = 0, sms = 148;
     cudaStream_t stream = nullptr;
-    int m = 0, n = 0;
-    bool maximize = false;
-    double obj_const = 0.0;
+    int count = 1;                        // instances
+    int m = 0, n = 0;                     // totals
+    std::vector<int> row_off, col_off, nnz_off;  // instance boundaries (count + 1)
+    DevBuf<int> d_row_off, d_col_off, d_nnz_off;
+    DevBuf<int> inst_row, inst_col;       // row / column -> instance (empty for one instance)
+    std::vector<char> maximize;
+    std::vector<double> obj_const;
     DevMat A, AT, Q;
     bool has_q = false, dplr = false;
     int qk = 0;
     DevBuf<int> perm, row_of, q_row_of;
     DevBuf<double> c, l, u, lo, hi, R, C, Rres, Cres;  // scaled FP64 data
     DevBuf<double> F64, D64;                            // scaled DPLR factor
-    DevBuf<double> scal;  // 0 bscale 1 cscale 2 normA 3 normQ 4 bnorm 5 cnorm 6 w0 7..9 power scratch
+    DevBuf<double> scal;                                // count x kScal per-instance scalars
+    std::vector<double> scal_host;
     DevBuf<double> red_partials;
     DevBuf<double> x64, y64, xr64, yr64, xo, yo;
-    DevBuf<double> work1, work2;  // n / m FP64 scratch
+    DevBuf<double> work1, work2;          // n / m FP64 scratch
+    DevBuf<double> ftx;                   // F^T x of the DPLR Hessian (2 x qk, FP64)
     VecSet<float> v32;
     VecSet<double> v64;
-    DevBuf<SolveState> st;
-    SolveState* st_host = nullptr;  // pinned mirror
+    DevBuf<SolveState> st;                // per instance
+    SolveState* st_host = nullptr;        // pinned mirror (count entries)
+    DevBuf<int> phase_flags;              // per-instance flags uploaded for a phase
+    int* phase_flags_host = nullptr;      // pinned
+    DevBuf<unsigned> arrive;              // k_eval arrival counter
     DevBuf<double> partials;
     std::unique_ptr<LevelGraph> graphs[3];
-    double scal_host[10] = {};
     double setup_seconds = 0.0;
-    long long launches = 0;  // kernel launches of the last solve
+    long long launches = 0;               // kernel launches of the last solve
+    std::vector<InstanceResult> results;
     bool solved = false;
+
+    const int* icol() const { return count > 1 ? inst_col.get() : nullptr; }
+    const int* irow() const { return count > 1 ? inst_row.get() : nullptr; }
 
     ~Problem() {
         for (auto& g : graphs) g.reset();
         if (st_host) cudaFreeHost(st_host);
+        if (phase_flags_host) cudaFreeHost(phase_flags_host);
         if (stream) cudaStreamDestroy(stream);
     }
 };

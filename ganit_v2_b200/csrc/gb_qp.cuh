@@ -17,6 +17,7 @@ template <class V>
 struct Store2Epi {
     V* __restrict__ y0;
     V* __restrict__ y1;
+    __device__ __forceinline__ bool begin(int) const { return true; }
     __device__ __forceinline__ NoPre prefetch(int) const { return {}; }
     __device__ __forceinline__ void operator()(int r, const V (&s)[2], const NoPre&) {
         y0[r] = s[0];

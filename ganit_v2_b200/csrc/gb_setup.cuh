@@ -69,6 +69,7 @@ inline void reduce_to(cudaStream_t s, long long n, F f, double* partials, double
 template <class V>
 struct StoreEpi {
     V* __restrict__ y;
+    __device__ __forceinline__ bool begin(int) const { return true; }
     __device__ __forceinline__ NoPre prefetch(int) const { return {}; }
     __device__ __forceinline__ void operator()(int r, const V (&s)[1], const NoPre&) { y[r] = s[0]; }
 };
@@ -138,12 +139,35 @@ static __global__ void k_fill(int n, double a, double* __restrict__ v) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = a;
 }
 
+// Per-instance scalars of a batch live in rows of kScal doubles.
+constexpr int kScal = 16;
+enum ScalIdx : int {
+    S_BSCALE = 0, S_CSCALE = 1, S_NORMA = 2, S_NORMQ = 3, S_BNORM = 4, S_CNORM = 5, S_W0 = 6,
+    S_PW_NORM = 7, S_PW_LAMBDA = 8, S_PW_STOP = 9, S_CN = 10, S_BN = 11, S_SIGN = 12, S_OBJC = 13
+};
+__device__ __forceinline__ int inst_of(const int* map, int i) { return map ? map[i] : 0; }
+
+// Segmented fixed-order reduction: CTA k folds f(i) over [off[k], off[k+1])
+// and writes post(sum) to out[k * kScal].
+template <class F, class P>
+__global__ void __launch_bounds__(kThreads) k_seg_red(const int* off, F f, double* out, P post) {
+    __shared__ double sh[kWarps];
+    const int k = blockIdx.x;
+    double acc = 0.0;
+    for (int i = off[k] + threadIdx.x; i < off[k + 1]; i += kThreads) acc += f(i);
+    double v[1] = {acc};
+    block_sum<1>(v, sh);
+    if (threadIdx.x == 0) post(v[0], out + static_cast<size_t>(k) * kScal);
+}
+
 // scaling.cpp:78-88: c' = sign c C, l' = l / C, u' = u / C, lo' = lo R, hi' = hi R
-static __global__ void k_scale_vectors(int n, int m, double sign, const double* c, const double* l, const double* u,
-                                const double* lo, const double* hi, const double* R, const double* Cs, double* cs_,
-                                double* ls, double* us, double* los, double* his) {
+static __global__ void k_scale_vectors(int n, int m, const int* inst_col, const double* sc, const double* c,
+                                       const double* l, const double* u, const double* lo, const double* hi,
+                                       const double* R, const double* Cs, double* cs_, double* ls, double* us,
+                                       double* los, double* his) {
     const int stride = gridDim.x * blockDim.x;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const double sign = sc[static_cast<size_t>(inst_of(inst_col, j)) * kScal + S_SIGN];
         cs_[j] = sign * c[j] * Cs[j];
         ls[j] = l[j] / Cs[j];
         us[j] = u[j] / Cs[j];
@@ -153,35 +177,38 @@ static __global__ void k_scale_vectors(int n, int m, double sign, const double* 
         his[i] = hi[i] * R[i];
     }
 }
-// scaling.cpp:89-101 (bscale / cscale live on the device at sc[0], sc[1])
-static __global__ void k_rescale(int n, int m, const double* sc, const double* R, const double* Cs, double* c, double* l,
-                          double* u, double* lo, double* hi, double* Rres, double* Cres) {
-    const double bscale = sc[0], cscale = sc[1];
+// scaling.cpp:89-101 (per-instance bscale / cscale)
+static __global__ void k_rescale(int n, int m, const int* inst_col, const int* inst_row, const double* sc,
+                                 const double* R, const double* Cs, double* c, double* l, double* u, double* lo,
+                                 double* hi, double* Rres, double* Cres) {
     const int stride = gridDim.x * blockDim.x;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const double* s = sc + static_cast<size_t>(inst_of(inst_col, j)) * kScal;
+        const double bscale = s[S_BSCALE], cscale = s[S_CSCALE];
         c[j] /= cscale;
         l[j] /= bscale;
         u[j] /= bscale;
         Cres[j] = Cs[j] / cscale;
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        const double bscale = sc[static_cast<size_t>(inst_of(inst_row, i)) * kScal + S_BSCALE];
         lo[i] /= bscale;
         hi[i] /= bscale;
         Rres[i] = R[i] / bscale;
     }
 }
-// CSR Hessian: Q'_ij = Q_ij * sign * C_i * C_j * bscale / cscale (scaling.cpp:104-107)
-static __global__ void k_scale_q(int nnz, const int* __restrict__ row_of, const int* __restrict__ idx, double sign,
-                          const double* __restrict__ Cs, const double* sc, double* __restrict__ val) {
-    const double bscale = sc[0], cscale = sc[1];
+// CSR Hessian (one instance): Q'_ij = Q_ij * sign * C_i * C_j * bscale / cscale (scaling.cpp:104-107)
+static __global__ void k_scale_q(int nnz, const int* __restrict__ row_of, const int* __restrict__ idx,
+                                 const double* __restrict__ Cs, const double* sc, double* __restrict__ val) {
+    const double bscale = sc[S_BSCALE], cscale = sc[S_CSCALE], sign = sc[S_SIGN];
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += gridDim.x * blockDim.x)
         val[p] *= sign * Cs[row_of[p]] * Cs[idx[p]] * bscale / cscale;
 }
-// DPLR Hessian Q = 2 (F F^T + diag D) scaled the same way:
+// DPLR Hessian Q = 2 (F F^T + diag D) scaled the same way (one instance):
 //   F'_jk = sqrt(bscale/cscale) C_j F_jk,  D'_j = (bscale/cscale) C_j^2 D_j.
-static __global__ void k_scale_dplr(int n, int k, const double* __restrict__ Cs, const double* sc, double* __restrict__ F,
-                             double* __restrict__ D) {
-    const double s2 = sc[0] / sc[1], s1 = sqrt(s2);
+static __global__ void k_scale_dplr(int n, int k, const double* __restrict__ Cs, const double* sc,
+                                    double* __restrict__ F, double* __restrict__ D) {
+    const double s2 = sc[S_BSCALE] / sc[S_CSCALE], s1 = sqrt(s2);
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)n * k;
          e += (long long)gridDim.x * blockDim.x) {
         const int j = static_cast<int>(e / k);
@@ -190,17 +217,48 @@ static __global__ void k_scale_dplr(int n, int k, const double* __restrict__ Cs,
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) D[j] *= s2 * Cs[j] * Cs[j];
 }
 
-// power-iteration step: if *nz > 0 (and not stopped): lambda = nz, v = z / nz; else stop.
-static __global__ void k_power_step(int n, const double* __restrict__ z, double* __restrict__ v, double* pw) {
-    // pw[0] = latest norm, pw[1] = lambda, pw[2] = stopped flag
-    const double nz = pw[0];
-    if (pw[2] != 0.0) return;
-    if (nz == 0.0) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) pw[2] = 1.0;
-        return;
+// Power iteration, per instance (scaling.cpp:137-152): v = z / ||z|| unless
+// the instance's iteration stopped or ||z|| == 0 ...
+static __global__ void k_power_vec(int n, const int* inst_col, const double* sc, const double* __restrict__ z,
+                                   double* __restrict__ v) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const double* s = sc + static_cast<size_t>(inst_of(inst_col, j)) * kScal;
+        const double nz = s[S_PW_NORM];
+        if (s[S_PW_STOP] == 0.0 && nz != 0.0) v[j] = z[j] / nz;
     }
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) v[j] = z[j] / nz;
-    if (blockIdx.x == 0 && threadIdx.x == 0) pw[1] = nz;
+}
+// ... then lambda = ||z|| ("if (nz == 0.0) break; lambda = nz").
+static __global__ void k_power_flags(int count, double* sc) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    double* s = sc + static_cast<size_t>(k) * kScal;
+    if (s[S_PW_STOP] != 0.0) return;
+    if (s[S_PW_NORM] == 0.0) s[S_PW_STOP] = 1.0;
+    else s[S_PW_LAMBDA] = s[S_PW_NORM];
+}
+static __global__ void k_power_reset(int count, double* sc) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    double* s = sc + static_cast<size_t>(k) * kScal;
+    s[S_PW_LAMBDA] = 0.0;
+    s[S_PW_STOP] = 0.0;
+}
+// ||A'|| = sqrt(lambda) * 1.01, or 1 for an instance without nonzeros
+// (scaling.cpp:132, 153-154); ||Q'|| = lambda * 1.01 (scaling.cpp:124).
+static __global__ void k_finish_norms(int count, const int* nnz_off, double* sc, int q) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    double* s = sc + static_cast<size_t>(k) * kScal;
+    if (q) s[S_NORMQ] = s[S_PW_LAMBDA] * 1.01;
+    else s[S_NORMA] = (nnz_off[k + 1] == nnz_off[k]) ? 1.0 : sqrt(s[S_PW_LAMBDA]) * 1.01;
+}
+// w0 = ||c'|| / ||b'||_finite (pdhg_impl.hpp:258-261)
+static __global__ void k_w0(int count, double* sc) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    double* s = sc + static_cast<size_t>(k) * kScal;
+    const double c = s[S_CN], b = s[S_BN];
+    s[S_W0] = (c > 1e-10 && b > 1e-10) ? c / b : 1.0;
 }
 
 // x0 = clamp(0, l, u), y0 = 0 (pdhg_impl.hpp:255-257)
@@ -220,12 +278,16 @@ __global__ void k_convert(long long n, const double* __restrict__ s, T* __restri
 }
 
 // x_orig = x' C bscale, y_orig = sign y' R cscale (pdhg_impl.hpp:310-314)
-static __global__ void k_unscale(int n, int m, double sign, const double* x, const double* y, const double* Cs,
-                          const double* R, const double* sc, double* xo, double* yo) {
-    const double bscale = sc[0], cscale = sc[1];
+static __global__ void k_unscale(int n, int m, const int* inst_col, const int* inst_row, const double* x,
+                                 const double* y, const double* Cs, const double* R, const double* sc, double* xo,
+                                 double* yo) {
     const int stride = gridDim.x * blockDim.x;
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) xo[j] = x[j] * Cs[j] * bscale;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) yo[i] = sign * y[i] * R[i] * cscale;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride)
+        xo[j] = x[j] * Cs[j] * sc[static_cast<size_t>(inst_of(inst_col, j)) * kScal + S_BSCALE];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        const double* s = sc + static_cast<size_t>(inst_of(inst_row, i)) * kScal;
+        yo[i] = s[S_SIGN] * y[i] * R[i] * s[S_CSCALE];
+    }
 }
 
 }  // namespace gb

@@ -41,13 +41,16 @@ struct alignas(16) RowBlock {
     int chunk, nchunks; // CHUNK: index and count
     int slot_base;      // CHUNK: first slot of the row
     int counter;        // CHUNK: arrival counter of the row
-    int pad0, pad1;
+    int inst;           // instance (batch member) the rows belong to
+    int pad1;
 };
 
 // Host: row-length-driven schedule.  `block_nnz` / `max_rows` are the
-// tunables (the batch autotuner varies them).
+// tunables (the batch autotuner varies them).  Blocks never straddle two
+// instances of a batch; seg_block[k] .. seg_block[k+1] are instance k's blocks.
 struct Schedule {
     std::vector<RowBlock> blocks;
+    std::vector<int> seg_block;
     int nslots = 0, ncounters = 0;
     int max_lg = 0;
 };
@@ -58,18 +61,18 @@ inline int floor_log2(int v) {
     return l;
 }
 
-// Walks the rows once and hands every block to `emit`; slot and counter ids
-// are numbered from *nslots / *ncounters on.
+// Walks rows [r_begin, r_end) once and hands every block to `emit`; slot and
+// counter ids are numbered from *nslots / *ncounters on; blocks get `inst`.
 template <class Emit>
-inline void schedule_rows(const int* ptr, int rows, int block_nnz, int max_rows, int* nslots, int* ncounters,
-                          Emit&& emit) {
-    int i = 0;
-    while (i < rows) {
+inline void schedule_rows(const int* ptr, int r_begin, int r_end, int block_nnz, int max_rows, int* nslots,
+                          int* ncounters, int inst, Emit&& emit) {
+    int i = r_begin;
+    while (i < r_end) {
         const int len = ptr[i + 1] - ptr[i];
         if (len > block_nnz) {
             if (len <= kLongSingle) {
                 RowBlock b{};
-                b.r0 = i; b.r1 = i + 1; b.p0 = ptr[i]; b.p1 = ptr[i + 1]; b.kind = kLong;
+                b.r0 = i; b.r1 = i + 1; b.p0 = ptr[i]; b.p1 = ptr[i + 1]; b.kind = kLong; b.inst = inst;
                 emit(b);
             } else {
                 const int nch = div_up(len, kChunkNnz);
@@ -79,7 +82,7 @@ inline void schedule_rows(const int* ptr, int rows, int block_nnz, int max_rows,
                     b.p0 = ptr[i] + c * kChunkNnz;
                     b.p1 = std::min(ptr[i + 1], b.p0 + kChunkNnz);
                     b.kind = kChunk; b.chunk = c; b.nchunks = nch;
-                    b.slot_base = *nslots; b.counter = *ncounters;
+                    b.slot_base = *nslots; b.counter = *ncounters; b.inst = inst;
                     emit(b);
                 }
                 *nslots += nch;
@@ -89,9 +92,9 @@ inline void schedule_rows(const int* ptr, int rows, int block_nnz, int max_rows,
             continue;
         }
         const int r0 = i, start = ptr[i];
-        while (i < rows && (i - r0) < max_rows && ptr[i + 1] - start <= block_nnz) ++i;
+        while (i < r_end && (i - r0) < max_rows && ptr[i + 1] - start <= block_nnz) ++i;
         RowBlock b{};
-        b.r0 = r0; b.r1 = i; b.p0 = start; b.p1 = ptr[i]; b.kind = kStream;
+        b.r0 = r0; b.r1 = i; b.p0 = start; b.p1 = ptr[i]; b.kind = kStream; b.inst = inst;
         const int nrows = i - r0;
         int g = kThreads / nrows;  // lanes available per row
         if (g > 32) g = 32;
@@ -100,26 +103,40 @@ inline void schedule_rows(const int* ptr, int rows, int block_nnz, int max_rows,
     }
 }
 
-inline Schedule build_schedule(const int* ptr, int rows, int block_nnz = kBlockNnz, int max_rows = kThreads) {
+// Schedule of a matrix whose rows are cut into `nseg` instances at
+// seg_off[0..nseg] (nseg = 1: one instance, rows [0, rows)).
+inline Schedule build_schedule(const int* ptr, int rows, const int* seg_off = nullptr, int nseg = 1,
+                               int block_nnz = kBlockNnz, int max_rows = kThreads) {
     Schedule s;
-    schedule_rows(ptr, rows, block_nnz, max_rows, &s.nslots, &s.ncounters, [&](const RowBlock& b) {
-        s.blocks.push_back(b);
-        s.max_lg = std::max(s.max_lg, b.lg);
-    });
+    s.seg_block.assign(nseg + 1, 0);
+    for (int k = 0; k < nseg; ++k) {
+        s.seg_block[k] = static_cast<int>(s.blocks.size());
+        const int r0 = seg_off ? seg_off[k] : 0, r1 = seg_off ? seg_off[k + 1] : rows;
+        schedule_rows(ptr, r0, r1, block_nnz, max_rows, &s.nslots, &s.ncounters, k, [&](const RowBlock& b) {
+            s.blocks.push_back(b);
+            s.max_lg = std::max(s.max_lg, b.lg);
+        });
+    }
+    s.seg_block[nseg] = static_cast<int>(s.blocks.size());
     return s;
 }
 
 // Device-resident schedule of one matrix.
 struct DevSchedule {
     DevBuf<RowBlock> blocks;
+    DevBuf<int> seg_block;  // per-instance block ranges
     DevBuf<double> slots;
     DevBuf<unsigned> counters;
     int nb = 0;
     int nslots = 0;
+    std::vector<int> host_seg_block;
     void upload(const Schedule& s, int nv_max, cudaStream_t st) {
         nb = static_cast<int>(s.blocks.size());
         blocks.reset(nb ? nb : 1);
         blocks.upload(s.blocks.data(), nb, st);
+        host_seg_block = s.seg_block;
+        seg_block.reset(host_seg_block.size());
+        seg_block.upload(host_seg_block.data(), host_seg_block.size(), st);
         nslots = s.nslots;
         slots.reset(static_cast<size_t>(s.nslots ? s.nslots : 1) * nv_max);
         counters.reset(s.ncounters ? s.ncounters : 1);
@@ -246,15 +263,17 @@ __device__ __forceinline__ void reduce_rows(const RowBlock& b, const V* prod, in
 }
 
 // CTA `cta` runs block `cta`.  Gather g(col, V(&)[NV]) supplies the NV vector
-// values of a column; epi.prefetch(row) loads a row's epilogue operands (issued
-// before the block's products) and epi(row, const V(&)[NV], pre) consumes a
-// finished row.
+// values of a column; epi.begin(inst) returns false to skip a block of an
+// instance that is not iterating (and loads per-instance scalars);
+// epi.prefetch(row) loads a row's epilogue operands (issued before the
+// block's products) and epi(row, const V(&)[NV], pre) consumes a finished row.
 template <int NV, class M, class V, class Gather, class Epi>
 __device__ __forceinline__ void spmv_run(const CsrView<M>& A, int cta, const Gather& g, Epi& epi,
                                          unsigned char* smem) {
     V* prod = reinterpret_cast<V*>(smem);
     V* red = reinterpret_cast<V*>(smem + sizeof(V) * NV * kProdStride);
     const RowBlock b = A.blocks[cta];
+    if (!epi.begin(b.inst)) return;  // instance not iterating (uniform over the CTA)
     if (b.kind != kStream) {
         long_block<NV, M, V>(A, b, g, epi, red);
         return;

@@ -1,0 +1,67 @@
+"""Batched solving (gb_batch_*): every instance of a batch behaves as if solved
+alone -- same verdict as the reference CPU PDHG (the oracle), FP64-certified
+KKT within tol, objective within 10 * tol, and at FP64 the per-instance
+iteration count within two checks of the oracle's."""
+import os
+
+import numpy as np
+import pytest
+
+from ganit_v2_b200 import workloads as W
+from tests.golden.make_golden import load_lp
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def mixed_batch():
+    lps = W.lp_batch(10, seed=500, m_min=30, m_max=400)
+    for name in ("rand_small", "infeasible", "rand_max", "rand_free", "blend_small"):
+        lps.append(load_lp(os.path.join(GOLD, name + ".npz"))[0])
+    return lps
+
+
+@pytest.fixture(scope="module")
+def batch():
+    return mixed_batch()
+
+
+@pytest.mark.parametrize("prec", ["double", "mixed"])
+def test_batch_matches_oracle_per_instance(batch, oracle_built, prec):
+    import ganit_v2_b200 as gb
+
+    P = {"double": gb.Precision.Double, "mixed": gb.Precision.Mixed}[prec]
+    with gb.BatchSolver(batch) as bs:
+        res = bs.solve(gb.Options(precision=P))
+        for i, (lp, r) in enumerate(zip(batch, res)):
+            o = oracle_built.solve(lp, precision=prec)
+            assert r.status_name == o.status, (i, lp.name)
+            if o.status == "OPTIMAL":
+                assert max(r.rel_primal, r.rel_dual, r.rel_gap) <= 1e-4 * 1.0000001, (i, lp.name)
+                assert abs(r.pobj - o.pobj) <= 1e-3 * (1 + abs(o.pobj)), (i, lp.name, r.pobj, o.pobj)
+            if prec == "double":
+                assert abs(r.iterations - o.iterations) <= 128, (i, lp.name, r.iterations, o.iterations)
+            x, y = r.x, r.y
+            assert x.shape == (lp.n,) and y.shape == (lp.m,) and np.all(np.isfinite(x))
+
+
+def test_batch_instance_equals_single_solve(batch):
+    """An instance inside a batch follows the same trajectory as alone."""
+    import ganit_v2_b200 as gb
+
+    with gb.BatchSolver(batch) as bs:
+        res = bs.solve(gb.Options(precision=gb.Precision.Double))
+    for i in (0, 3, len(batch) - 1):
+        single = gb.solve_pdhg_gpu(batch[i], gb.Options(precision=gb.Precision.Double))
+        assert single.status == res[i].status
+        assert abs(single.iterations - res[i].iterations) <= 64
+        assert abs(single.pobj - res[i].pobj) <= 1e-6 * (1 + abs(single.pobj))
+
+
+def test_batch_schedule_report(batch):
+    import ganit_v2_b200 as gb
+
+    with gb.BatchSolver(batch[:4]) as bs:
+        s = bs.schedule()
+    assert s["threads"] == 256 and s["blocks_per_sm"] >= 1
+    assert len(s["groups_A"]) == 4 and all(g in (1, 2, 4, 8, 16, 32) for g in s["groups_A"])
