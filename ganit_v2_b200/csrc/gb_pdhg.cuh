@@ -467,31 +467,56 @@ __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalA
     }
     __syncthreads();
     if (!am_last) return;
-    // last CTA: each thread reduces whole instances (their blocks, in block
-    // order) and runs their decisions
+    // Last CTA: reduce every instance's partials in a fixed order and run its
+    // decision.  An instance with many blocks is reduced by the whole CTA
+    // (one at a time), the others by one warp each.
     __threadfence();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int any_active = 0;
-    for (int k = threadIdx.x; k < a.count; k += kThreads) {
-        SolveState& s = a.st[k];
-        if (!eval_includes(s, a.mode)) {
-            s.ran_body = 0;
-            continue;
-        }
-        double T[kTerms];
+    auto load_terms = [&](int k, int first, int step, double (&T)[kTerms]) {
 #pragma unroll
         for (int q = 0; q < kTerms; ++q) T[q] = 0.0;
-        for (int b = a.seg_a[k]; b < a.seg_a[k + 1]; ++b) {
+        const int a0 = a.seg_a[k], a1 = a.seg_a[k + 1], t0 = a.seg_t[k], t1 = a.seg_t[k + 1];
+        const int na = a1 - a0, nt = t1 - t0;
+        for (int i = first; i < na + nt; i += step) {
+            const size_t b = i < na ? static_cast<size_t>(a0 + i) : static_cast<size_t>(nbA + t0 + i - na);
 #pragma unroll
-            for (int q = 0; q < kTerms; ++q) T[q] += __ldcg(a.partials + static_cast<size_t>(b) * kTerms + q);
+            for (int q = 0; q < kTerms; ++q) T[q] += __ldcg(a.partials + b * kTerms + q);
         }
-        for (int b = a.seg_t[k]; b < a.seg_t[k + 1]; ++b) {
-#pragma unroll
-            for (int q = 0; q < kTerms; ++q)
-                T[q] += __ldcg(a.partials + static_cast<size_t>(nbA + b) * kTerms + q);
-        }
+    };
+    auto finish = [&](SolveState& s, const double (&T)[kTerms]) {
         s.ran_body = (a.mode == kEvalCheck) ? 1 : 0;
         decide(s, T, a.mode);
         any_active |= s.active;
+    };
+    constexpr int kWide = 128;  // blocks above which an instance gets the whole CTA
+    for (int k = 0; k < a.count; ++k) {
+        const int nblk = (a.seg_a[k + 1] - a.seg_a[k]) + (a.seg_t[k + 1] - a.seg_t[k]);
+        if (nblk <= kWide) continue;
+        SolveState& s = a.st[k];
+        if (!eval_includes(s, a.mode)) {
+            if (threadIdx.x == 0) s.ran_body = 0;
+            continue;
+        }
+        double T[kTerms];
+        load_terms(k, threadIdx.x, kThreads, T);
+        block_sum<kTerms>(T, red);
+        if (threadIdx.x == 0) finish(s, T);
+        __syncthreads();
+    }
+    for (int k = wid; k < a.count; k += kWarps) {
+        const int nblk = (a.seg_a[k + 1] - a.seg_a[k]) + (a.seg_t[k + 1] - a.seg_t[k]);
+        if (nblk > kWide) continue;
+        SolveState& s = a.st[k];
+        if (!eval_includes(s, a.mode)) {
+            if (lane == 0) s.ran_body = 0;
+            continue;
+        }
+        double T[kTerms];
+        load_terms(k, lane, 32, T);
+#pragma unroll
+        for (int q = 0; q < kTerms; ++q) T[q] = warp_sum(T[q]);
+        if (lane == 0) finish(s, T);
     }
     any_active = __syncthreads_or(any_active);
     if (threadIdx.x == 0) {
