@@ -3,12 +3,13 @@
 Public API (mirrors include/ganit/pdhg.hpp of the reference):
 ``Options``, ``Precision``, ``Status``, ``Result``, ``solve_pdhg_gpu`` (alias
 ``solve_pdhg_b200``), plus ``Problem`` (resident problem), ``Backend``
-(Backend-concept operations), ``BatchSolver`` and ``DiffBatch``.
+(Backend-concept operations), ``BatchSolver`` and ``DiffSolver`` (with the
+``torch.autograd.Function`` wrapper in :mod:`ganit_v2_b200.diff`).
 The compute path is libganit_b200.so (sm_100a); there is no CPU fallback.
 """
 from .lp import LP, Csr
-from .api import (Backend, BatchSolver, GanitError, Options, Precision, Problem, Result, Status, load_library, set_device,
+from .api import (Backend, BatchSolver, DiffSolver, GanitError, Options, Precision, Problem, Result, Status, load_library, set_device,
                   solve_pdhg_b200, solve_pdhg_gpu, LIB_PATH)
 
-__all__ = ["LP", "Csr", "Backend", "BatchSolver", "GanitError", "Options", "Precision", "Problem", "Result", "Status",
+__all__ = ["LP", "Csr", "Backend", "BatchSolver", "DiffSolver", "GanitError", "Options", "Precision", "Problem", "Result", "Status",
            "load_library", "set_device", "solve_pdhg_b200", "solve_pdhg_gpu", "LIB_PATH"]

@@ -128,6 +128,18 @@ class GbKktScalars(C.Structure):
     _fields_ = [("obj_scale", C.c_double), ("obj_const", C.c_double), ("bnorm", C.c_double), ("cnorm", C.c_double)]
 
 
+class _GbDiffOptions(C.Structure):
+    _fields_ = [("implicit_max_iters", C.c_int64), ("implicit_tol", C.c_double), ("polish", C.c_int32),
+                ("pad", C.c_int32)]
+
+
+class _GbDiffInfo(C.Structure):
+    _fields_ = [("tau", C.c_double), ("sigma", C.c_double), ("tail_iterations", C.c_int64),
+                ("checkpoint_every", C.c_int64), ("implicit_iterations", C.c_int64), ("implicit_residual", C.c_double),
+                ("implicit_converged", C.c_int32), ("free_cols", C.c_int32), ("active_rows", C.c_int32),
+                ("polished", C.c_int32), ("polish_iterations", C.c_int64), ("launches", C.c_int64)]
+
+
 class GbKkt(C.Structure):
     _fields_ = [("pobj", C.c_double), ("dobj", C.c_double), ("rel_p", C.c_double), ("rel_d", C.c_double),
                 ("rel_gap", C.c_double), ("err", C.c_double)]
@@ -142,7 +154,8 @@ EXPORTS = [
     "gb_spmv_AT", "gb_spmv_Q", "gb_primal_step", "gb_dual_step", "gb_sub", "gb_scale_into", "gb_primal_res2",
     "gb_dual_res", "gb_row_dual_obj", "gb_dot", "gb_dot_c", "gb_diff2", "gb_batch_create", "gb_batch_solve",
     "gb_batch_get_solution", "gb_batch_schedule", "gb_batch_destroy", "gb_diff_create", "gb_diff_forward",
-    "gb_diff_backward", "gb_diff_destroy", "gb_eval_kkt_noalloc",
+    "gb_diff_default_options", "gb_diff_set_options", "gb_diff_backward", "gb_diff_get_info", "gb_diff_tail_start", "gb_diff_destroy",
+    "gb_eval_kkt_noalloc",
 ]
 
 _lib = None
@@ -176,8 +189,10 @@ def load_library(path: str = LIB_PATH):
         "gb_batch_create": (i32, [i32, vp, vp, vp]), "gb_batch_solve": (i32, [vp, vp, vp]),
         "gb_batch_get_solution": (i32, [vp, i32, vp, vp]), "gb_batch_schedule": (i32, [vp, vp, vp, vp]),
         "gb_batch_destroy": (None, [vp]), "gb_diff_create": (i32, [i32, vp, vp, i32, i32, vp]),
-        "gb_diff_forward": (i32, [vp, vp, vp, vp, vp]),
-        "gb_diff_backward": (i32, [vp, vp, vp, vp, vp, vp, vp]), "gb_diff_destroy": (None, [vp]),
+        "gb_diff_forward": (i32, [vp, vp, vp, vp, vp]), "gb_diff_default_options": (None, [vp]),
+        "gb_diff_set_options": (i32, [vp, vp]),
+        "gb_diff_backward": (i32, [vp, vp, vp, vp, vp, vp, vp]), "gb_diff_get_info": (i32, [vp, i32, vp]),
+        "gb_diff_tail_start": (i32, [vp, vp, vp]), "gb_diff_destroy": (None, [vp]),
         "gb_eval_kkt_noalloc": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
@@ -371,6 +386,99 @@ class BatchSolver:
     def close(self):
         if getattr(self, "_h", None):
             self._lib.gb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class DiffSolver:
+    """Differentiable batch of LPs (gb_diff_*).
+
+    ``forward`` solves every instance with restarted PDHG to ``opt.tol`` and
+    then runs ``tail_iters`` (K) plain FP64 PDHG iterations, checkpointed every
+    ``ckpt_every`` (R); its outputs are the last tail iterate.  ``backward``
+    maps dL/dx*, dL/dy* to dL/dc, dL/dlo, dL/dhi and dL/d(A values) by exact
+    reverse mode through the K tail iterations plus the implicit completion
+    at the tail start (``implicit_iters`` MINRES steps at most, relative
+    residual ``implicit_tol``; ``implicit_iters=0`` gives the truncated
+    gradient).  With ``polish`` the tail starts from the vertex of the active
+    set the solver's point identifies, when that vertex certifies better.
+    All vectors are the concatenation of the instances' vectors.  LPs must
+    not use a Hessian."""
+
+    def __init__(self, lps, opt: Options | None = None, tail_iters: int = 200, ckpt_every: int = 20,
+                 implicit_iters: int = 20000, implicit_tol: float = 1e-10, polish: bool = True):
+        self._lib = load_library()
+        self.lps = list(lps)
+        self._views = [_LpView(lp) for lp in self.lps]
+        arr = (_GbLp * len(self._views))(*[v.s for v in self._views])
+        o = _opts(opt)
+        h = C.c_void_p()
+        _check(self._lib.gb_diff_create(len(self._views), arr, C.addressof(o), int(tail_iters), int(ckpt_every),
+                                        C.byref(h)))
+        self._h = h
+        self.n_off = np.concatenate([[0], np.cumsum([lp.n for lp in self.lps])]).astype(np.int64)
+        self.m_off = np.concatenate([[0], np.cumsum([lp.m for lp in self.lps])]).astype(np.int64)
+        self.nnz_off = np.concatenate([[0], np.cumsum([lp.A.nnz for lp in self.lps])]).astype(np.int64)
+        self.set_options(implicit_iters, implicit_tol, polish)
+
+    def __len__(self):
+        return len(self.lps)
+
+    def set_options(self, implicit_iters: int = 20000, implicit_tol: float = 1e-10, polish: bool = True):
+        o = _GbDiffOptions(int(implicit_iters), float(implicit_tol), int(bool(polish)), 0)
+        _check(self._lib.gb_diff_set_options(self._h, C.byref(o)))
+
+    def forward(self, opt: Options | None = None):
+        """Returns (results, x, y): per-instance results and the concatenated x*, y*."""
+        o = _opts(opt)
+        res = (_GbResult * len(self.lps))()
+        x = np.zeros(int(self.n_off[-1]))
+        y = np.zeros(int(self.m_off[-1]))
+        _check(self._lib.gb_diff_forward(self._h, C.addressof(o), res, _p(x), _p(y)))
+        out = [_result(r, x[self.n_off[i]:self.n_off[i + 1]], y[self.m_off[i]:self.m_off[i + 1]])
+               for i, r in enumerate(res)]
+        return out, x, y
+
+    def backward(self, dl_dx=None, dl_dy=None) -> dict:
+        """Returns {"c", "lo", "hi", "a_val"} gradients (concatenated)."""
+        gx = None if dl_dx is None else np.ascontiguousarray(dl_dx, dtype=np.float64)
+        gy = None if dl_dy is None else np.ascontiguousarray(dl_dy, dtype=np.float64)
+        if gx is not None and gx.shape != (int(self.n_off[-1]),):
+            raise ValueError("dl_dx must have the total column count")
+        if gy is not None and gy.shape != (int(self.m_off[-1]),):
+            raise ValueError("dl_dy must have the total row count")
+        out = {"c": np.zeros(int(self.n_off[-1])), "lo": np.zeros(int(self.m_off[-1])),
+               "hi": np.zeros(int(self.m_off[-1])), "a_val": np.zeros(int(self.nnz_off[-1]))}
+        _check(self._lib.gb_diff_backward(self._h, _p(gx), _p(gy), _p(out["c"]), _p(out["lo"]), _p(out["hi"]),
+                                          _p(out["a_val"])))
+        return out
+
+    def info(self, i: int) -> dict:
+        r = _GbDiffInfo()
+        _check(self._lib.gb_diff_get_info(self._h, int(i), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in _GbDiffInfo._fields_ if k != "pad"}
+
+    def tail_start(self):
+        """Scaled start point (x, y) of the tail iterations (concatenated)."""
+        x = np.zeros(int(self.n_off[-1]))
+        y = np.zeros(int(self.m_off[-1]))
+        _check(self._lib.gb_diff_tail_start(self._h, _p(x), _p(y)))
+        return x, y
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.gb_diff_destroy(self._h)
             self._h = None
 
     def __del__(self):

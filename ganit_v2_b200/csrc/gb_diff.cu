@@ -1,10 +1,934 @@
-// Differentiable solving (gb_diff_*): implementation pending.
-#include "../../include/ganit_b200.h"
-#include "gb_common.cuh"
-namespace gb { extern thread_local std::string g_last_error; }
-extern "C" {
-int gb_diff_create(int, const gb_lp*, const gb_options*, int, int, gb_diff**) { gb::g_last_error = "not built yet"; return GB_ERR_UNSUPPORTED; }
-int gb_diff_forward(gb_diff*, const gb_options*, gb_result*, double*, double*) { return GB_ERR_UNSUPPORTED; }
-int gb_diff_backward(gb_diff*, const double*, const double*, double*, double*, double*, double*) { return GB_ERR_UNSUPPORTED; }
-void gb_diff_destroy(gb_diff*) {}
+// Differentiable batched LP layer (gb_diff_*).  No counterpart in the
+// reference: it differentiates the restarted PDHG of src/pdhg_impl.hpp.
+//
+// Forward (gb_diff_forward)
+//   1. The batch engine solves every instance to opt->tol (gb_engine.cu).
+//   2. A tail of K plain PDHG iterations (src/pdhg_impl.hpp:133-139 with the
+//      final step sizes tau = eta / w, sigma = eta w, no restart check) runs
+//      from the returned point.  Its state is checkpointed every R
+//      iterations; the last iterate z_K = (x_K, y_K) is the layer's output and
+//      is certified again in FP64.
+// Backward (gb_diff_backward), FP64 on the scaled problem
+//   3. Exact reverse mode through the K tail iterations: segment by segment
+//      (last first) the R iterations are recomputed from their checkpoint,
+//      keeping iterates and projection codes, then reversed step by step:
+//        k_rev_cols  A^T pass: adjoint of the primal step (projection mask,
+//                    extrapolation xbar = 2x+ - x), accumulates dL/dc
+//        k_rev_da    dL/dA_ij -= sigma lq_i xbar_j + y_i lg_j
+//        k_rev_rows  A pass: adjoint of the dual step (projection mask),
+//                    accumulates dL/dlo, dL/dhi
+//   4. Implicit completion.  The tail start z_0 is (to the solve tolerance) a
+//      fixed point z = T(z; theta) of the PDHG map, so its own dependence on
+//      theta adds (dT/dtheta)^T nu with nu = (I - J0^T)^{-1} mu_0, where mu_0 is
+//      the adjoint left at z_0 and J0 the Jacobian of T there.  With the
+//      projection masks of z_0 (free columns F, dual-active rows D) that
+//      fixed point reduces exactly to
+//          B^T p = mu_x[F],   B q = mu_y[D],   B = A'[D, F],
+//      i.e. one symmetric indefinite system [[0, B^T], [B, 0]] (q; p) =
+//      (mu_x; mu_y), solved per instance by MINRES (Paige & Saunders, SIAM J.
+//      Numer. Anal. 12, 1975) on the same SpMV kernels.  Then dc' += q,
+//      d(lo|hi)' += p, dA' -= p xbar^T + y q^T.  For a nondegenerate vertex B
+//      is the optimal basis matrix and this is the basis sensitivity; plain
+//      unrolling would need O(cond(B)^2) iterations to get there.  With the
+//      completion switched off (gb_diff_set_implicit(d, 0, .)) the result is
+//      the gradient of the K-step map with z_0 held fixed.
+//   5. Gradients go back through the scaling of src/scaling.cpp:75-101 with
+//      the scaling factors held constant.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+
+#include "gb_problem.cuh"
+
+namespace gb {
+namespace {
+
+using i8 = int8_t;
+
+// ---------------------------------------------------------------- forward tail
+// x+ = clamp(x - tau (c - A^T y), l, u), xbar = 2 x+ - x (backend_cpu.cpp:67-80);
+// code 1 = strictly inside the box (derivative 1), 0 / 2 = clamped low / high.
+struct TailColEpi {
+    const double* __restrict__ x;
+    const double* __restrict__ c;
+    const double* __restrict__ l;
+    const double* __restrict__ u;
+    const double* __restrict__ tau;
+    double* __restrict__ xn;
+    double* __restrict__ xb;
+    i8* __restrict__ code;
+    double t;
+    __device__ __forceinline__ bool begin(int inst) {
+        t = tau[inst];
+        return true;
+    }
+    __device__ __forceinline__ NoPre prefetch(int) const { return {}; }
+    __device__ __forceinline__ void operator()(int j, const double (&s)[1], const NoPre&) {
+        const double xj = x[j], lj = l[j], uj = u[j];
+        const double z = xj - t * (c[j] - s[0]);
+        const double xp = z < lj ? lj : (z > uj ? uj : z);
+        xn[j] = xp;
+        xb[j] = 2.0 * xp - xj;
+        code[j] = (z > lj && z < uj) ? i8(1) : (z <= lj ? i8(0) : i8(2));
+    }
+};
+
+// q = y - sigma A xbar, y+ = q + clamp(-q, sigma lo, sigma hi) (backend_cpu.cpp:81-92);
+// code 0 = -q inside [sigma lo, sigma hi] (y+ = 0), 1 / 2 = clamped to lo / hi.
+struct TailRowEpi {
+    const double* __restrict__ y;
+    const double* __restrict__ lo;
+    const double* __restrict__ hi;
+    const double* __restrict__ sig;
+    double* __restrict__ yn;
+    i8* __restrict__ code;
+    double s_;
+    __device__ __forceinline__ bool begin(int inst) {
+        s_ = sig[inst];
+        return true;
+    }
+    __device__ __forceinline__ NoPre prefetch(int) const { return {}; }
+    __device__ __forceinline__ void operator()(int i, const double (&s)[1], const NoPre&) {
+        const double q = y[i] - s_ * s[0];
+        const double t = -q, a = s_ * lo[i], b = s_ * hi[i];
+        if (t < a) {
+            yn[i] = q + a;
+            code[i] = 1;
+        } else if (t > b) {
+            yn[i] = q + b;
+            code[i] = 2;
+        } else {
+            yn[i] = q + t;
+            code[i] = 0;
+        }
+    }
+};
+
+__global__ void __launch_bounds__(kThreads) k_tail_cols(const __grid_constant__ CsrView<double> AT,
+                                                        const double* __restrict__ y, TailColEpi e) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    TailColEpi epi = e;
+    spmv_run<1, double, double>(AT, blockIdx.x, GatherOne<double>{y}, epi, smem);
 }
+__global__ void __launch_bounds__(kThreads) k_tail_rows(const __grid_constant__ CsrView<double> A,
+                                                        const double* __restrict__ xb, TailRowEpi e) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    TailRowEpi epi = e;
+    spmv_run<1, double, double>(A, blockIdx.x, GatherOne<double>{xb}, epi, smem);
+}
+
+// ---------------------------------------------------------------- reverse pass
+// Adjoint of one iteration, given lx, ly (adjoints of x+, y+) and
+// lq = [code_y != 0] ly:
+//   lxbar = -sigma A^T lq;  lz = [code_x == 1] (lx + 2 lxbar);
+//   lx <- lz - lxbar;  lg = -tau lz (= dL/dc contribution);  ly <- lq - A lg.
+struct RevColEpi {
+    const i8* __restrict__ code;
+    const double* __restrict__ tau;
+    const double* __restrict__ sig;
+    double* __restrict__ lx;
+    double* __restrict__ lg;
+    double* __restrict__ gc;
+    double t, s_;
+    __device__ __forceinline__ bool begin(int inst) {
+        t = tau[inst];
+        s_ = sig[inst];
+        return true;
+    }
+    __device__ __forceinline__ NoPre prefetch(int) const { return {}; }
+    __device__ __forceinline__ void operator()(int j, const double (&s)[1], const NoPre&) {
+        const double lxb = -s_ * s[0];
+        const double ltot = lx[j] + 2.0 * lxb;
+        const double lz = code[j] == 1 ? ltot : 0.0;
+        lx[j] = lz - lxb;
+        const double g = -t * lz;
+        lg[j] = g;
+        gc[j] += g;
+    }
+};
+
+// ly = lq - (A lg)_i; when the previous step of the segment exists its lq and
+// bound gradients are formed right away (same row, same thread).
+struct RevRowEpi {
+    const i8* __restrict__ code_prev;
+    const double* __restrict__ sig;
+    double* __restrict__ lq;
+    double* __restrict__ ly;
+    double* __restrict__ glo;
+    double* __restrict__ ghi;
+    double s_;
+    __device__ __forceinline__ bool begin(int inst) {
+        s_ = sig[inst];
+        return true;
+    }
+    __device__ __forceinline__ NoPre prefetch(int) const { return {}; }
+    __device__ __forceinline__ void operator()(int i, const double (&s)[1], const NoPre&) {
+        const double l = lq[i] - s[0];
+        ly[i] = l;
+        if (code_prev) {
+            const int c = code_prev[i];
+            lq[i] = c ? l : 0.0;
+            if (c == 1) glo[i] += s_ * l;
+            else if (c == 2) ghi[i] += s_ * l;
+        }
+    }
+};
+
+__global__ void __launch_bounds__(kThreads) k_rev_cols(const __grid_constant__ CsrView<double> AT,
+                                                       const double* __restrict__ lq, RevColEpi e) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    RevColEpi epi = e;
+    spmv_run<1, double, double>(AT, blockIdx.x, GatherOne<double>{lq}, epi, smem);
+}
+__global__ void __launch_bounds__(kThreads) k_rev_rows(const __grid_constant__ CsrView<double> A,
+                                                       const double* __restrict__ lg, RevRowEpi e) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    RevRowEpi epi = e;
+    spmv_run<1, double, double>(A, blockIdx.x, GatherOne<double>{lg}, epi, smem);
+}
+
+// lq = [code != 0] ly and the bound gradients of the step whose dual codes are `code`.
+__global__ void k_rev_start(int m, const int* __restrict__ inst_row, const i8* __restrict__ code,
+                            const double* __restrict__ sig, const double* __restrict__ ly, double* __restrict__ lq,
+                            double* __restrict__ glo, double* __restrict__ ghi) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const int c = code[i];
+        const double l = ly[i];
+        lq[i] = c ? l : 0.0;
+        const double s = sig[inst_of(inst_row, i)];
+        if (c == 1) glo[i] += s * l;
+        else if (c == 2) ghi[i] += s * l;
+    }
+}
+
+// dL/dA'_e of one iteration: g = c - A^T y and q = y - sigma A xbar both read A.
+__global__ void k_rev_da(int nnz, const int* __restrict__ row_of, const int* __restrict__ idx,
+                         const int* __restrict__ inst_row, const double* __restrict__ sig,
+                         const double* __restrict__ lq, const double* __restrict__ xb, const double* __restrict__ y,
+                         const double* __restrict__ lg, double* __restrict__ ga) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += gridDim.x * blockDim.x) {
+        const int i = row_of[e], j = idx[e];
+        const double s = sig[inst_of(inst_row, i)];
+        ga[e] -= s * lq[i] * xb[j] + y[i] * lg[j];
+    }
+}
+
+// ---------------------------------------------------------------- implicit completion (MINRES)
+struct alignas(16) MrState {
+    double beta1, beta, cs, sn, dbar, epsln, phibar, tol;
+    long long it, max_it;
+    int done, converged, free_cols, active_rows;
+};
+
+struct MrVecs {
+    const int* col_off;
+    const int* row_off;
+    const i8* cx;  // column codes of z_0 (1 = free)
+    const i8* cy;  // row codes of z_0 (!= 0 = dual active)
+    double *vx, *vy, *vpx, *vpy, *px, *py, *d1x, *d1y, *d2x, *d2y, *sx, *sy;
+    MrState* st;
+};
+
+// Right-hand side (mu_x on free columns; mu_y on dual-active rows), v_1 = b / beta_1.
+__global__ void __launch_bounds__(kThreads) k_mr_init(const __grid_constant__ MrVecs a, const double* __restrict__ mux,
+                                                      const double* __restrict__ muy, long long max_it, double tol) {
+    __shared__ double red[kWarps * 3];
+    __shared__ double inv;
+    const int k = blockIdx.x;
+    const int c0 = a.col_off[k], c1 = a.col_off[k + 1], r0 = a.row_off[k], r1 = a.row_off[k + 1];
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int j = c0 + threadIdx.x; j < c1; j += kThreads) {
+        const bool f = a.cx[j] == 1;
+        const double b = f ? mux[j] : 0.0;
+        a.vx[j] = b;
+        a.vpx[j] = a.px[j] = a.d1x[j] = a.d2x[j] = a.sx[j] = 0.0;
+        v[0] += b * b;
+        v[1] += f ? 1.0 : 0.0;
+    }
+    for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
+        const bool d = a.cy[i] != 0;
+        const double b = d ? muy[i] : 0.0;
+        a.vy[i] = b;
+        a.vpy[i] = a.py[i] = a.d1y[i] = a.d2y[i] = a.sy[i] = 0.0;
+        v[0] += b * b;
+        v[2] += d ? 1.0 : 0.0;
+    }
+    block_sum<3>(v, red);
+    if (threadIdx.x == 0) {
+        MrState s;
+        memset(&s, 0, sizeof(s));
+        s.beta1 = sqrt(v[0]);
+        s.beta = s.beta1;
+        s.cs = -1.0;
+        s.phibar = s.beta1;
+        s.tol = tol;
+        s.free_cols = static_cast<int>(v[1]);
+        s.active_rows = static_cast<int>(v[2]);
+        // In exact arithmetic MINRES ends within dim = |F| + |D| steps; finite
+        // precision Lanczos needs a few times that on consistent systems, and an
+        // inconsistent one (a wrong active set) never converges.
+        s.max_it = min(max_it, 4LL * (s.free_cols + s.active_rows) + 100);
+        s.converged = s.beta1 == 0.0;
+        s.done = s.converged || max_it <= 0;
+        a.st[k] = s;
+        inv = s.beta1 > 0.0 ? 1.0 / s.beta1 : 0.0;
+    }
+    __syncthreads();
+    const double iv = inv;
+    for (int j = c0 + threadIdx.x; j < c1; j += kThreads) a.vx[j] *= iv;
+    for (int i = r0 + threadIdx.x; i < r1; i += kThreads) a.vy[i] *= iv;
+}
+
+// p = K v with K = [[0, B^T], [B, 0]] in the full index space (zero outside the masks).
+struct MrEpi {
+    const i8* __restrict__ code;
+    double* __restrict__ out;
+    const MrState* __restrict__ st;
+    int cols;
+    __device__ __forceinline__ bool begin(int inst) const { return st[inst].done == 0; }
+    __device__ __forceinline__ NoPre prefetch(int) const { return {}; }
+    __device__ __forceinline__ void operator()(int r, const double (&s)[1], const NoPre&) {
+        const int c = code[r];
+        out[r] = (cols ? c == 1 : c != 0) ? s[0] : 0.0;
+    }
+};
+struct MrOpArgs {
+    CsrView<double> A, AT;
+    MrVecs v;
+};
+__global__ void __launch_bounds__(kThreads) k_mr_op(const __grid_constant__ MrOpArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (static_cast<int>(blockIdx.x) < a.A.nb) {
+        MrEpi e{a.v.cy, a.v.py, a.v.st, 0};
+        spmv_run<1, double, double>(a.A, blockIdx.x, GatherOne<double>{a.v.vx}, e, smem);
+    } else {
+        MrEpi e{a.v.cx, a.v.px, a.v.st, 1};
+        spmv_run<1, double, double>(a.AT, blockIdx.x - a.A.nb, GatherOne<double>{a.v.vy}, e, smem);
+    }
+}
+
+// One MINRES step per instance (one CTA per instance; fixed-order reductions):
+// Lanczos (alpha, beta), the two Givens rotations, direction and solution update.
+__global__ void __launch_bounds__(kThreads) k_mr_update(const __grid_constant__ MrVecs a) {
+    __shared__ double red[kWarps];
+    __shared__ double bc[6];
+    const int k = blockIdx.x;
+    MrState* sp = a.st + k;
+    if (sp->done) return;
+    const int c0 = a.col_off[k], c1 = a.col_off[k + 1], r0 = a.row_off[k], r1 = a.row_off[k + 1];
+    double v[1] = {0.0};
+    for (int j = c0 + threadIdx.x; j < c1; j += kThreads) v[0] += a.vx[j] * a.px[j];
+    for (int i = r0 + threadIdx.x; i < r1; i += kThreads) v[0] += a.vy[i] * a.py[i];
+    block_sum<1>(v, red);
+    if (threadIdx.x == 0) bc[0] = v[0];
+    __syncthreads();
+    const double alpha = bc[0], beta = sp->beta;
+    v[0] = 0.0;
+    for (int j = c0 + threadIdx.x; j < c1; j += kThreads) {
+        const double p = a.px[j] - alpha * a.vx[j] - beta * a.vpx[j];
+        a.px[j] = p;
+        v[0] += p * p;
+    }
+    for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
+        const double p = a.py[i] - alpha * a.vy[i] - beta * a.vpy[i];
+        a.py[i] = p;
+        v[0] += p * p;
+    }
+    block_sum<1>(v, red);
+    if (threadIdx.x == 0) {
+        MrState s = *sp;
+        const double bn = sqrt(v[0]);
+        const double oldeps = s.epsln;
+        const double delta = s.cs * s.dbar + s.sn * alpha;
+        const double gbar = s.sn * s.dbar - s.cs * alpha;
+        s.epsln = s.sn * bn;
+        s.dbar = -s.cs * bn;
+        double gamma = sqrt(gbar * gbar + bn * bn);
+        if (!(gamma > 1e-300)) gamma = 1e-300;
+        s.cs = gbar / gamma;
+        s.sn = bn / gamma;
+        const double phi = s.cs * s.phibar;
+        s.phibar = s.sn * s.phibar;
+        s.beta = bn;
+        s.it += 1;
+        s.converged = (s.phibar <= s.tol * s.beta1) || !(bn > 1e-300);
+        s.done = s.converged || s.it >= s.max_it || !isfinite(s.phibar);
+        *sp = s;
+        bc[1] = phi;
+        bc[2] = 1.0 / gamma;
+        bc[3] = oldeps;
+        bc[4] = delta;
+        bc[5] = bn > 1e-300 ? 1.0 / bn : 0.0;
+    }
+    __syncthreads();
+    const double phi = bc[1], ig = bc[2], oldeps = bc[3], delta = bc[4], ib = bc[5];
+    for (int j = c0 + threadIdx.x; j < c1; j += kThreads) {
+        const double w = (a.vx[j] - oldeps * a.d2x[j] - delta * a.d1x[j]) * ig;
+        a.d2x[j] = a.d1x[j];
+        a.d1x[j] = w;
+        a.sx[j] += phi * w;
+        a.vpx[j] = a.vx[j];
+        a.vx[j] = a.px[j] * ib;
+    }
+    for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
+        const double w = (a.vy[i] - oldeps * a.d2y[i] - delta * a.d1y[i]) * ig;
+        a.d2y[i] = a.d1y[i];
+        a.d1y[i] = w;
+        a.sy[i] += phi * w;
+        a.vpy[i] = a.vy[i];
+        a.vy[i] = a.py[i] * ib;
+    }
+}
+
+// Parameter gradient of T at z_0 against nu: dc' += q, d(lo|hi)' += p, dA' -= p xbar0^T + y0 q^T.
+__global__ void k_implicit_grads(int n, int m, int nnz, const int* __restrict__ row_of, const int* __restrict__ idx,
+                                 const i8* __restrict__ cy, const double* __restrict__ q, const double* __restrict__ p,
+                                 const double* __restrict__ xb0, const double* __restrict__ y0, double* __restrict__ gc,
+                                 double* __restrict__ glo, double* __restrict__ ghi, double* __restrict__ ga) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) gc[j] += q[j];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        const int c = cy[i];
+        if (c == 1) glo[i] += p[i];
+        else if (c == 2) ghi[i] += p[i];
+    }
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += stride) {
+        const int i = row_of[e], j = idx[e];
+        ga[e] -= p[i] * xb0[j] + y0[i] * q[j];
+    }
+}
+
+// ---------------------------------------------------------------- solution polishing
+// Reduced KKT system of the active set read off one PDHG step (codes):
+//   B^T y_D = c'_F,  B x_F = bnd_D - A'[D, N] x_N,
+// x_N at the bound its code names, bnd the row bound its code names.
+__global__ void k_polish_rhs_cols(int n, const i8* __restrict__ cx, const double* __restrict__ c,
+                                  const double* __restrict__ l, const double* __restrict__ u, double* __restrict__ rhs_x,
+                                  double* __restrict__ xn) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const int k = cx[j];
+        rhs_x[j] = k == 1 ? c[j] : 0.0;
+        xn[j] = k == 1 ? 0.0 : (k == 0 ? l[j] : u[j]);
+    }
+}
+struct PolishRowEpi {
+    const i8* __restrict__ cy;
+    const double* __restrict__ lo;
+    const double* __restrict__ hi;
+    double* __restrict__ rhs_y;
+    __device__ __forceinline__ bool begin(int) const { return true; }
+    __device__ __forceinline__ NoPre prefetch(int) const { return {}; }
+    __device__ __forceinline__ void operator()(int i, const double (&s)[1], const NoPre&) {
+        const int k = cy[i];
+        rhs_y[i] = k == 0 ? 0.0 : (k == 1 ? lo[i] : hi[i]) - s[0];
+    }
+};
+__global__ void __launch_bounds__(kThreads) k_polish_rhs_rows(const __grid_constant__ CsrView<double> A,
+                                                              const double* __restrict__ xn, PolishRowEpi e) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    PolishRowEpi epi = e;
+    spmv_run<1, double, double>(A, blockIdx.x, GatherOne<double>{xn}, epi, smem);
+}
+// Polished point of the instances in `use` (others keep (x, y)); x_F is
+// clamped into its box so that a wrong active set shows in the FP64 KKT.
+__global__ void k_polish_point(int n, int m, const int* inst_col, const int* inst_row, const int* __restrict__ use,
+                               const i8* __restrict__ cx, const i8* __restrict__ cy, const double* __restrict__ sol_x,
+                               const double* __restrict__ sol_y, const double* __restrict__ l,
+                               const double* __restrict__ u, double* __restrict__ x, double* __restrict__ y) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        if (!use[inst_of(inst_col, j)]) continue;
+        const int k = cx[j];
+        const double lj = l[j], uj = u[j];
+        if (k == 1) {
+            const double v = sol_x[j];
+            x[j] = v < lj ? lj : (v > uj ? uj : v);
+        } else {
+            x[j] = k == 0 ? lj : uj;
+        }
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride)
+        if (use[inst_of(inst_row, i)]) y[i] = cy[i] != 0 ? sol_y[i] : 0.0;
+}
+// (x, y) <- (xs, ys) on the instances in `restore`.
+__global__ void k_restore(int n, int m, const int* inst_col, const int* inst_row, const int* __restrict__ restore,
+                          const double* __restrict__ xs, const double* __restrict__ ys, double* __restrict__ x,
+                          double* __restrict__ y) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride)
+        if (restore[inst_of(inst_col, j)]) x[j] = xs[j];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride)
+        if (restore[inst_of(inst_row, i)]) y[i] = ys[i];
+}
+
+// ---------------------------------------------------------------- scaling of adjoints and gradients
+// x = x' C bscale, y = sign y' R cscale  =>  dL/dx' = dL/dx C bscale, dL/dy' = sign dL/dy R cscale.
+__global__ void k_adjoint_in(int n, int m, const int* inst_col, const int* inst_row, const double* __restrict__ sc,
+                             const double* __restrict__ Cs, const double* __restrict__ R, const double* __restrict__ gx,
+                             const double* __restrict__ gy, double* __restrict__ lx, double* __restrict__ ly) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride)
+        lx[j] = gx[j] * Cs[j] * sc[static_cast<size_t>(inst_of(inst_col, j)) * kScal + S_BSCALE];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        const double* s = sc + static_cast<size_t>(inst_of(inst_row, i)) * kScal;
+        ly[i] = s[S_SIGN] * gy[i] * R[i] * s[S_CSCALE];
+    }
+}
+// c' = sign c C / cscale, lo' = lo R / bscale, hi' = hi R / bscale, A' = R A C.
+__global__ void k_grads_out(int n, int m, int nnz, const int* inst_col, const int* inst_row,
+                            const int* __restrict__ row_of, const int* __restrict__ idx, const double* __restrict__ sc,
+                            const double* __restrict__ Cs, const double* __restrict__ R, const double* __restrict__ gc,
+                            const double* __restrict__ glo, const double* __restrict__ ghi,
+                            const double* __restrict__ ga, double* __restrict__ oc, double* __restrict__ olo,
+                            double* __restrict__ ohi, double* __restrict__ oa) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const double* s = sc + static_cast<size_t>(inst_of(inst_col, j)) * kScal;
+        oc[j] = s[S_SIGN] * gc[j] * Cs[j] / s[S_CSCALE];
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        const double b = sc[static_cast<size_t>(inst_of(inst_row, i)) * kScal + S_BSCALE];
+        olo[i] = glo[i] * R[i] / b;
+        ohi[i] = ghi[i] * R[i] / b;
+    }
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += stride) oa[e] = ga[e] * R[row_of[e]] * Cs[idx[e]];
+}
+
+
+constexpr int kMrChunk = 64;  // MINRES steps between host looks at the per-instance flags
+
+}  // namespace
+
+// ---------------------------------------------------------------- host object
+struct Diff {
+    std::unique_ptr<Problem> P;
+    int K = 200, R = 20, nseg = 10;
+    long long mr_max = 20000;
+    double mr_tol = 1e-10;
+    bool polish = true;
+    std::vector<double> tau_h, sig_h;
+    DevBuf<double> tau, sig;
+    DevBuf<double> ck_x, ck_y;      // nseg checkpoints (x, y)
+    DevBuf<double> sx, sy, sxb;     // iterates of one segment: (R+1) n, (R+1) m, R n
+    DevBuf<i8> scx, scy;            // projection codes of one segment: R n, R m
+    int seg_valid = -1;             // segment whose iterates the buffers hold
+    DevBuf<double> lx, ly, lq, lg, gc, glo, ghi, ga;
+    DevBuf<double> mr[12];
+    DevBuf<MrState> mst;
+    MrState* mst_host = nullptr;
+    DevBuf<int> flags;              // per-instance selection (polish use / restore)
+    int* flags_host = nullptr;
+    DevBuf<double> io_n, io_m, io_m2, io_z;
+    std::vector<gb_diff_info> info;
+    bool forward_done = false;
+    bool backward_done = false;
+    long long launches = 0;
+
+    ~Diff() {
+        if (mst_host) cudaFreeHost(mst_host);
+        if (flags_host) cudaFreeHost(flags_host);
+    }
+
+    size_t n() const { return static_cast<size_t>(P->n); }
+    size_t m() const { return static_cast<size_t>(P->m); }
+    size_t nnz() const { return static_cast<size_t>(P->A.nnz); }
+    double* x_at(int k) { return sx.get() + k * n(); }
+    double* y_at(int k) { return sy.get() + k * m(); }
+    double* xb_at(int k) { return sxb.get() + k * n(); }
+    i8* cx_at(int k) { return scx.get() + k * n(); }
+    i8* cy_at(int k) { return scy.get() + k * m(); }
+
+    MrVecs mr_vecs() {
+        MrVecs v;
+        v.col_off = P->d_col_off.get();
+        v.row_off = P->d_row_off.get();
+        v.cx = cx_at(0);
+        v.cy = cy_at(0);
+        v.vx = mr[0].get(); v.vy = mr[1].get(); v.vpx = mr[2].get(); v.vpy = mr[3].get();
+        v.px = mr[4].get(); v.py = mr[5].get(); v.d1x = mr[6].get(); v.d1y = mr[7].get();
+        v.d2x = mr[8].get(); v.d2y = mr[9].get(); v.sx = mr[10].get(); v.sy = mr[11].get();
+        v.st = mst.get();
+        return v;
+    }
+
+    // `steps` iterations from (sx[0], sy[0]) keeping iterates and codes.
+    void run_segment(int steps) {
+        Problem& p = *P;
+        cudaStream_t s = p.stream;
+        const size_t smem = spmv_smem_bytes<1, double>();
+        const CsrView<double> A = p.A.view<double>(), AT = p.AT.view<double>();
+        for (int k = 0; k < steps; ++k) {
+            if (AT.nb) {
+                TailColEpi e{x_at(k), p.c.get(), p.l.get(), p.u.get(), tau.get(), x_at(k + 1), xb_at(k), cx_at(k), 0.0};
+                k_tail_cols<<<AT.nb, kThreads, smem, s>>>(AT, y_at(k), e);
+            }
+            if (A.nb) {
+                TailRowEpi e{y_at(k), p.lo.get(), p.hi.get(), sig.get(), y_at(k + 1), cy_at(k), 0.0};
+                k_tail_rows<<<A.nb, kThreads, smem, s>>>(A, xb_at(k), e);
+            }
+            launches += 2;
+        }
+    }
+    void recompute(int seg) {
+        cudaStream_t s = P->stream;
+        GB_CUDA(cudaMemcpyAsync(x_at(0), ck_x.get() + seg * n(), n() * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        GB_CUDA(cudaMemcpyAsync(y_at(0), ck_y.get() + seg * m(), m() * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        run_segment(R);
+        seg_valid = seg;
+    }
+
+    // Per-instance MINRES on K = [[0, B^T], [B, 0]] with B = A'[D, F] read from
+    // the codes of step 0 of the resident segment; solution in mr[10], mr[11];
+    // per-instance state left in mst_host.
+    void minres(const double* rhs_x, const double* rhs_y) {
+        Problem& p = *P;
+        cudaStream_t s = p.stream;
+        const size_t smem = spmv_smem_bytes<1, double>();
+        MrVecs v = mr_vecs();
+        k_mr_init<<<p.count, kThreads, 0, s>>>(v, rhs_x, rhs_y, mr_max, mr_tol);
+        launches += 1;
+        MrOpArgs oa{p.A.view<double>(), p.AT.view<double>(), v};
+        const int nb = oa.A.nb + oa.AT.nb;
+        long long steps = 0;
+        while (steps < mr_max) {
+            for (int c = 0; c < kMrChunk; ++c) {
+                if (nb) k_mr_op<<<nb, kThreads, smem, s>>>(oa);
+                k_mr_update<<<p.count, kThreads, 0, s>>>(v);
+            }
+            launches += 2 * kMrChunk;
+            steps += kMrChunk;
+            GB_CUDA(cudaMemcpyAsync(mst_host, mst.get(), sizeof(MrState) * p.count, cudaMemcpyDeviceToHost, s));
+            GB_CUDA(cudaStreamSynchronize(s));
+            bool any = false;
+            for (int k = 0; k < p.count; ++k) any |= mst_host[k].done == 0;
+            if (!any) break;
+        }
+        GB_CUDA(cudaMemcpyAsync(mst_host, mst.get(), sizeof(MrState) * p.count, cudaMemcpyDeviceToHost, s));
+        GB_CUDA(cudaStreamSynchronize(s));
+    }
+};
+
+void diff_alloc(Diff& D) {
+    Problem& P = *D.P;
+    const size_t n = std::max<size_t>(D.n(), 1), m = std::max<size_t>(D.m(), 1), z = std::max<size_t>(D.nnz(), 1);
+    D.tau.reset(P.count);
+    D.sig.reset(P.count);
+    D.ck_x.reset(n * D.nseg);
+    D.ck_y.reset(m * D.nseg);
+    D.sx.reset(n * (D.R + 1));
+    D.sy.reset(m * (D.R + 1));
+    D.sxb.reset(n * D.R);
+    D.scx.reset(n * D.R);
+    D.scy.reset(m * D.R);
+    for (DevBuf<double>* b : {&D.lx, &D.lg, &D.gc, &D.io_n}) b->reset(n);
+    for (DevBuf<double>* b : {&D.ly, &D.lq, &D.glo, &D.ghi, &D.io_m, &D.io_m2}) b->reset(m);
+    D.ga.reset(z);
+    D.io_z.reset(z);
+    for (int k = 0; k < 12; ++k) D.mr[k].reset(k % 2 == 0 ? n : m);
+    D.mst.reset(P.count);
+    D.flags.reset(P.count);
+    GB_CUDA(cudaMallocHost(&D.mst_host, sizeof(MrState) * P.count));
+    GB_CUDA(cudaMallocHost(&D.flags_host, sizeof(int) * P.count));
+    D.info.assign(P.count, gb_diff_info{});
+}
+
+inline double kkt_err(const Kkt& k) {
+    const double e = std::max(k.rel_p, std::max(k.rel_d, k.rel_gap));
+    return std::isfinite(e) ? e : INFINITY;
+}
+
+// Polishing (the reduced KKT solve of OSQP-style solvers): per instance,
+// replace the PDHG point by the vertex of the active set one PDHG step reads
+// off it, when that vertex certifies better in FP64.
+void polish(Diff& D) {
+    Problem& P = *D.P;
+    cudaStream_t s = P.stream;
+    const int n = P.n, m = P.m;
+    const size_t nb = D.n() * sizeof(double), mb = D.m() * sizeof(double);
+    const int gv = elem_grid(std::max(n, m), P.sms);
+    std::vector<double> err0(P.count);
+    for (int k = 0; k < P.count; ++k) err0[k] = kkt_err(P.st_host[k].kcert);
+    // PDHG point -> sx[0], sy[0]; one step for the codes
+    GB_CUDA(cudaMemcpyAsync(D.x_at(0), P.x64.get(), nb, cudaMemcpyDeviceToDevice, s));
+    GB_CUDA(cudaMemcpyAsync(D.y_at(0), P.y64.get(), mb, cudaMemcpyDeviceToDevice, s));
+    D.run_segment(1);
+    D.seg_valid = -1;
+    double* rhs_x = D.lx.get();   // adjoint buffers are free during the forward
+    double* rhs_y = D.ly.get();
+    double* xn = D.lg.get();
+    k_polish_rhs_cols<<<gv, kThreads, 0, s>>>(n, D.cx_at(0), P.c.get(), P.l.get(), P.u.get(), rhs_x, xn);
+    if (P.A.sched.nb) {
+        PolishRowEpi e{D.cy_at(0), P.lo.get(), P.hi.get(), rhs_y};
+        k_polish_rhs_rows<<<P.A.sched.nb, kThreads, spmv_smem_bytes<1, double>(), s>>>(P.A.view<double>(), xn, e);
+    }
+    D.launches += 2;
+    D.minres(rhs_x, rhs_y);
+    for (int k = 0; k < P.count; ++k) {
+        D.flags_host[k] = D.mst_host[k].converged ? 1 : 0;
+        D.info[k].polish_iterations = D.mst_host[k].it;
+    }
+    D.flags.upload(D.flags_host, P.count, s);
+    k_polish_point<<<gv, kThreads, 0, s>>>(n, m, P.icol(), P.irow(), D.flags.get(), D.cx_at(0), D.cy_at(0),
+                                          D.mr[10].get(), D.mr[11].get(), P.l.get(), P.u.get(), P.x64.get(),
+                                          P.y64.get());
+    certify(P);
+    bool any_restore = false;
+    for (int k = 0; k < P.count; ++k) {
+        const bool keep = D.flags_host[k] && kkt_err(P.st_host[k].kcert) < err0[k];
+        D.info[k].polished = keep ? 1 : 0;
+        D.flags_host[k] = keep ? 0 : 1;
+        any_restore |= !keep;
+    }
+    if (any_restore) {
+        D.flags.upload(D.flags_host, P.count, s);
+        k_restore<<<gv, kThreads, 0, s>>>(n, m, P.icol(), P.irow(), D.flags.get(), D.x_at(0), D.y_at(0), P.x64.get(),
+                                         P.y64.get());
+        D.launches += 1;
+    }
+    D.launches += 3;
+}
+
+void diff_forward(Diff& D, const gb_options* opt, gb_result* res, double* x_out, double* y_out) {
+    Problem& P = *D.P;
+    cudaStream_t s = P.stream;
+    std::vector<gb_result> tmp(P.count);
+    gb_result* r = res ? res : tmp.data();
+    solve_problem(P, opt, r);
+    D.launches = P.launches;
+    D.info.assign(P.count, gb_diff_info{});
+    // tail step sizes from the final primal weight (pdhg_impl.hpp:87-91, LP)
+    D.tau_h.resize(P.count);
+    D.sig_h.resize(P.count);
+    for (int k = 0; k < P.count; ++k) {
+        const SolveState& st = P.st_host[k];
+        D.tau_h[k] = st.eta / st.w;
+        D.sig_h[k] = st.eta * st.w;
+    }
+    D.tau.upload(D.tau_h.data(), P.count, s);
+    D.sig.upload(D.sig_h.data(), P.count, s);
+    if (D.polish) polish(D);
+    const size_t nb = D.n() * sizeof(double), mb = D.m() * sizeof(double);
+    GB_CUDA(cudaMemcpyAsync(D.x_at(0), P.x64.get(), nb, cudaMemcpyDeviceToDevice, s));
+    GB_CUDA(cudaMemcpyAsync(D.y_at(0), P.y64.get(), mb, cudaMemcpyDeviceToDevice, s));
+    for (int seg = 0; seg < D.nseg; ++seg) {
+        if (seg > 0) {
+            GB_CUDA(cudaMemcpyAsync(D.x_at(0), D.x_at(D.R), nb, cudaMemcpyDeviceToDevice, s));
+            GB_CUDA(cudaMemcpyAsync(D.y_at(0), D.y_at(D.R), mb, cudaMemcpyDeviceToDevice, s));
+        }
+        GB_CUDA(cudaMemcpyAsync(D.ck_x.get() + seg * D.n(), D.x_at(0), nb, cudaMemcpyDeviceToDevice, s));
+        GB_CUDA(cudaMemcpyAsync(D.ck_y.get() + seg * D.m(), D.y_at(0), mb, cudaMemcpyDeviceToDevice, s));
+        D.run_segment(D.R);
+    }
+    D.seg_valid = D.nseg - 1;
+    // the layer's output z_K, certified in FP64 and unscaled
+    GB_CUDA(cudaMemcpyAsync(P.x64.get(), D.x_at(D.R), nb, cudaMemcpyDeviceToDevice, s));
+    GB_CUDA(cudaMemcpyAsync(P.y64.get(), D.y_at(D.R), mb, cudaMemcpyDeviceToDevice, s));
+    certify(P);
+    k_unscale<<<elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s>>>(P.n, P.m, P.icol(), P.irow(), P.x64.get(),
+                                                                     P.y64.get(), P.C.get(), P.R.get(), P.scal.get(),
+                                                                     P.xo.get(), P.yo.get());
+    D.launches += 2;
+    if (x_out) GB_CUDA(cudaMemcpyAsync(x_out, P.xo.get(), nb, cudaMemcpyDeviceToHost, s));
+    if (y_out) GB_CUDA(cudaMemcpyAsync(y_out, P.yo.get(), mb, cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaStreamSynchronize(s));
+    GB_CUDA(cudaGetLastError());
+    for (int k = 0; k < P.count; ++k) {
+        const Kkt& f = P.st_host[k].kcert;
+        const double sign = P.maximize[k] ? -1.0 : 1.0;
+        r[k].pobj = sign * f.pobj;
+        r[k].dobj = sign * f.dobj;
+        r[k].rel_primal = f.rel_p;
+        r[k].rel_dual = f.rel_d;
+        r[k].rel_gap = f.rel_gap;
+        r[k].iterations += D.K;
+        if (r[k].status == GB_OPTIMAL &&
+            !(f.rel_p <= opt->tol * 1.0000001 && f.rel_d <= opt->tol * 1.0000001 && f.rel_gap <= opt->tol * 1.0000001))
+            r[k].status = GB_NUMERICAL_ERROR;
+        gb_diff_info& in = D.info[k];
+        in.tau = D.tau_h[k];
+        in.sigma = D.sig_h[k];
+        in.tail_iterations = D.K;
+        in.checkpoint_every = D.R;
+        in.free_cols = in.active_rows = -1;
+    }
+    D.forward_done = true;
+    D.backward_done = false;
+}
+
+void diff_backward(Diff& D, const double* dl_dx, const double* dl_dy, double* dl_dc, double* dl_dlo, double* dl_dhi,
+                   double* dl_dval) {
+    GB_REQUIRE(D.forward_done, "gb_diff_backward before gb_diff_forward");
+    Problem& P = *D.P;
+    cudaStream_t s = P.stream;
+    const int n = P.n, m = P.m, nnz = static_cast<int>(P.A.nnz);
+    const size_t nb = D.n() * sizeof(double), mb = D.m() * sizeof(double);
+    const int gv = elem_grid(std::max(n, m), P.sms), gz = elem_grid(std::max<long long>(nnz, 1), P.sms);
+    const int gall = elem_grid(std::max<long long>(std::max(n, m), nnz), P.sms);
+    D.launches = 0;
+    // upstream adjoint in scaled space
+    if (dl_dx) D.io_n.upload(dl_dx, D.n(), s);
+    else GB_CUDA(cudaMemsetAsync(D.io_n.get(), 0, nb, s));
+    if (dl_dy) D.io_m.upload(dl_dy, D.m(), s);
+    else GB_CUDA(cudaMemsetAsync(D.io_m.get(), 0, mb, s));
+    k_adjoint_in<<<gv, kThreads, 0, s>>>(n, m, P.icol(), P.irow(), P.scal.get(), P.C.get(), P.R.get(), D.io_n.get(),
+                                         D.io_m.get(), D.lx.get(), D.ly.get());
+    GB_CUDA(cudaMemsetAsync(D.gc.get(), 0, nb, s));
+    GB_CUDA(cudaMemsetAsync(D.glo.get(), 0, mb, s));
+    GB_CUDA(cudaMemsetAsync(D.ghi.get(), 0, mb, s));
+    GB_CUDA(cudaMemsetAsync(D.ga.get(), 0, D.ga.size() * sizeof(double), s));
+    D.launches += 1;
+
+    // 3. reverse through the tail, last segment first
+    const size_t smem = spmv_smem_bytes<1, double>();
+    const CsrView<double> A = P.A.view<double>(), AT = P.AT.view<double>();
+    for (int seg = D.nseg - 1; seg >= 0; --seg) {
+        if (seg != D.seg_valid) D.recompute(seg);
+        k_rev_start<<<gv, kThreads, 0, s>>>(m, P.irow(), D.cy_at(D.R - 1), D.sig.get(), D.ly.get(), D.lq.get(),
+                                            D.glo.get(), D.ghi.get());
+        D.launches += 1;
+        for (int k = D.R - 1; k >= 0; --k) {
+            if (AT.nb) {
+                RevColEpi e{D.cx_at(k), D.tau.get(), D.sig.get(), D.lx.get(), D.lg.get(), D.gc.get(), 0.0, 0.0};
+                k_rev_cols<<<AT.nb, kThreads, smem, s>>>(AT, D.lq.get(), e);
+            }
+            if (nnz)
+                k_rev_da<<<gz, kThreads, 0, s>>>(nnz, P.row_of.get(), P.A.idx.get(), P.irow(), D.sig.get(),
+                                                 D.lq.get(), D.xb_at(k), D.y_at(k), D.lg.get(), D.ga.get());
+            if (A.nb) {
+                RevRowEpi e{k > 0 ? D.cy_at(k - 1) : nullptr, D.sig.get(), D.lq.get(), D.ly.get(), D.glo.get(),
+                            D.ghi.get(), 0.0};
+                k_rev_rows<<<A.nb, kThreads, smem, s>>>(A, D.lg.get(), e);
+            }
+            D.launches += 3;
+        }
+    }
+    // (lx, ly) now hold mu_0, the adjoint at the tail start; segment 0's step 0 is resident.
+
+    // 4. implicit completion
+    if (D.mr_max > 0) {
+        D.minres(D.lx.get(), D.ly.get());
+        k_implicit_grads<<<gall, kThreads, 0, s>>>(n, m, nnz, P.row_of.get(), P.A.idx.get(), D.cy_at(0),
+                                                   D.mr[10].get(), D.mr[11].get(), D.xb_at(0), D.y_at(0),
+                                                   D.gc.get(), D.glo.get(), D.ghi.get(), D.ga.get());
+        D.launches += 1;
+        for (int k = 0; k < P.count; ++k) {
+            const MrState& st = D.mst_host[k];
+            gb_diff_info& in = D.info[k];
+            in.implicit_iterations = st.it;
+            in.implicit_residual = st.beta1 > 0.0 ? st.phibar / st.beta1 : 0.0;
+            in.implicit_converged = st.converged;
+            in.free_cols = st.free_cols;
+            in.active_rows = st.active_rows;
+        }
+    }
+
+    // 5. back to the original data
+    k_grads_out<<<gall, kThreads, 0, s>>>(n, m, nnz, P.icol(), P.irow(), P.row_of.get(), P.A.idx.get(), P.scal.get(),
+                                          P.C.get(), P.R.get(), D.gc.get(), D.glo.get(), D.ghi.get(), D.ga.get(),
+                                          D.io_n.get(), D.io_m.get(), D.io_m2.get(), D.io_z.get());
+    D.launches += 1;
+    if (dl_dc) GB_CUDA(cudaMemcpyAsync(dl_dc, D.io_n.get(), nb, cudaMemcpyDeviceToHost, s));
+    if (dl_dlo) GB_CUDA(cudaMemcpyAsync(dl_dlo, D.io_m.get(), mb, cudaMemcpyDeviceToHost, s));
+    if (dl_dhi) GB_CUDA(cudaMemcpyAsync(dl_dhi, D.io_m2.get(), mb, cudaMemcpyDeviceToHost, s));
+    if (dl_dval && nnz) GB_CUDA(cudaMemcpyAsync(dl_dval, D.io_z.get(), D.nnz() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaStreamSynchronize(s));
+    GB_CUDA(cudaGetLastError());
+    D.backward_done = true;
+}
+
+}  // namespace gb
+
+struct gb_diff {
+    std::unique_ptr<gb::Diff> d;
+};
+
+extern "C" {
+
+void gb_diff_default_options(gb_diff_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->implicit_max_iters = 20000;
+    o->implicit_tol = 1e-10;
+    o->polish = 1;
+}
+
+int gb_diff_create(int count, const gb_lp* lps, const gb_options* opt, int tail_iters, int ckpt_every,
+                   gb_diff** out) {
+    return gb::guarded([&] {
+        GB_REQUIRE(out != nullptr, "out is NULL");
+        *out = nullptr;
+        GB_REQUIRE(count >= 1 && lps != nullptr, "need at least one problem");
+        GB_REQUIRE(tail_iters >= 1 && ckpt_every >= 1 && tail_iters % ckpt_every == 0,
+                   "tail_iters must be a positive multiple of ckpt_every");
+        for (int k = 0; k < count; ++k)
+            GB_REQUIRE(lps[k].q_ptr == nullptr && lps[k].q_rank == 0, "the differentiable layer takes LPs only");
+        gb_options o;
+        if (opt) o = *opt;
+        else gb_default_options(&o);
+        auto D = std::make_unique<gb::Diff>();
+        D->P.reset(gb::create_problem(count, lps, &o));
+        D->K = tail_iters;
+        D->R = ckpt_every;
+        D->nseg = tail_iters / ckpt_every;
+        gb::diff_alloc(*D);
+        *out = new gb_diff{std::move(D)};
+    });
+}
+
+int gb_diff_set_options(gb_diff* d, const gb_diff_options* o) {
+    return gb::guarded([&] {
+        GB_REQUIRE(d != nullptr && o != nullptr, "null argument");
+        GB_REQUIRE(o->implicit_max_iters >= 0 && o->implicit_tol > 0.0,
+                   "implicit_max_iters must be >= 0 and implicit_tol > 0");
+        d->d->mr_max = o->implicit_max_iters;
+        d->d->mr_tol = o->implicit_tol;
+        d->d->polish = o->polish != 0;
+    });
+}
+
+int gb_diff_forward(gb_diff* d, const gb_options* opt, gb_result* results, double* x_out, double* y_out) {
+    return gb::guarded([&] {
+        GB_REQUIRE(d != nullptr, "null handle");
+        gb_options o;
+        if (opt) o = *opt;
+        else gb_default_options(&o);
+        GB_CUDA(cudaSetDevice(d->d->P->device));
+        gb::diff_forward(*d->d, &o, results, x_out, y_out);
+    });
+}
+
+int gb_diff_backward(gb_diff* d, const double* dl_dx, const double* dl_dy, double* dl_dc, double* dl_dlo,
+                     double* dl_dhi, double* dl_dval) {
+    return gb::guarded([&] {
+        GB_REQUIRE(d != nullptr, "null handle");
+        GB_CUDA(cudaSetDevice(d->d->P->device));
+        gb::diff_backward(*d->d, dl_dx, dl_dy, dl_dc, dl_dlo, dl_dhi, dl_dval);
+    });
+}
+
+int gb_diff_get_info(gb_diff* d, int i, gb_diff_info* out) {
+    return gb::guarded([&] {
+        GB_REQUIRE(d != nullptr && out != nullptr, "null argument");
+        gb::Diff& D = *d->d;
+        GB_REQUIRE(i >= 0 && i < D.P->count, "instance index out of range");
+        GB_REQUIRE(D.forward_done, "no forward pass yet");
+        *out = D.info[i];
+        out->launches = D.launches;
+    });
+}
+
+int gb_diff_tail_start(gb_diff* d, double* x_scaled, double* y_scaled) {
+    return gb::guarded([&] {
+        GB_REQUIRE(d != nullptr, "null handle");
+        gb::Diff& D = *d->d;
+        GB_REQUIRE(D.forward_done, "no forward pass yet");
+        cudaStream_t s = D.P->stream;
+        if (x_scaled) GB_CUDA(cudaMemcpyAsync(x_scaled, D.ck_x.get(), D.n() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (y_scaled) GB_CUDA(cudaMemcpyAsync(y_scaled, D.ck_y.get(), D.m() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        GB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+void gb_diff_destroy(gb_diff* d) { delete d; }
+
+}  // extern "C"

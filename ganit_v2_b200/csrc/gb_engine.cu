@@ -20,23 +20,6 @@ namespace gb {
 thread_local std::string g_last_error;
 thread_local int g_device = 0;
 
-template <class F>
-int guarded(F&& f) {
-    try {
-        f();
-        return GB_OK;
-    } catch (const Error& e) {
-        g_last_error = e.what();
-        return e.code;
-    } catch (const std::bad_alloc&) {
-        g_last_error = "host allocation failed";
-        return GB_ERR_NOMEM;
-    } catch (const std::exception& e) {
-        g_last_error = e.what();
-        return GB_ERR_INVALID;
-    }
-}
-
 inline void check_device(int dev, int* sms) {
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) throw Error(GB_ERR_NODEVICE, "no CUDA device");

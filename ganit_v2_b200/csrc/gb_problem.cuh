@@ -126,4 +126,28 @@ struct Problem {
     }
 };
 
+// Engine entry points (gb_engine.cu) shared with the differentiable layer.
+extern thread_local std::string g_last_error;
+Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt);
+void solve_problem(Problem& P, const gb_options* opt, gb_result* res);
+void certify(Problem& P);  // FP64 KKT of (x64, y64) of every instance into st_host[k].kcert
+
+// Runs f, turning exceptions into the ABI's status codes (message in g_last_error).
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return GB_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return GB_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return GB_ERR_INVALID;
+    }
+}
+
 }  // namespace gb

@@ -15,6 +15,10 @@ for the random feasible LPs the engine is measured on:
   diagonal-plus-low-rank form or in the lifted form of
   bench/gen_portfolio.py:4-8 that the reference can read.
 * :func:`lp_batch` -- many random feasible LPs of log-uniform size.
+* :func:`nondegenerate_lp` / :func:`diff_batch` -- random LPs of the same
+  shape whose optimum is a unique, strictly complementary vertex (the
+  instances on which solution derivatives exist and equal basis
+  sensitivities).
 
 Dual sign convention (reference backend_cpu.cpp:73, 81-92): the reduced cost is
 ``c - A^T y``, so the dual of a ``<=`` row is <= 0.
@@ -239,6 +243,89 @@ def lp_batch(count: int = 512, seed: int = 1000, m_min: int = 50, m_max: int = 4
         k = np.minimum(k, m)
         out.append(random_feasible_lp(m, n, k, seed=seed + i, name=f"batch{i}_m{m}_n{n}"))
     return out
+
+
+def nondegenerate_lp(m: int = 500, n: int = 1000, nnz_per_col: int = 10, seed: int = 0, ub: float = 10.0,
+                     eq_frac: float = 0.5, tight_frac: float = 0.8, max_cond: float | None = None,
+                     name: str | None = None) -> LP:
+    """Random LP whose optimum (x0, y0) is a nondegenerate vertex.
+
+    Same matrix family as :func:`random_feasible_lp` (N(0,1) values, a fixed
+    count of distinct random rows per column, boxes [0, ub], the first
+    ``eq_frac`` of the rows equalities, the rest ``<=``).  That generator makes
+    every column with x0 strictly inside its box carry zero reduced cost, so
+    its optimal face has dimension (#interior - #tight rows), about 200 at
+    m=500, n=1000, and the solution map has no derivative.  Here instead:
+
+    * ``tight`` rows: all equalities and a ``tight_frac`` share of the ``<=``
+      rows, whose duals y0 are nonzero (<= -0.1 on ``<=`` rows); the other
+      ``<=`` rows get y0 = 0 and slack U(0.1, 1);
+    * exactly #tight columns are interior, x0 ~ U(0.1 ub, 0.9 ub); the rest
+      sit at 0 or ub with reduced costs |s0| ~ U(0.1, 1) of the right sign;
+    * the basis matrix A[tight, interior] is checked nonsingular by a sparse
+      LU and the draw is repeated (same stream) otherwise; with ``max_cond``
+      set, draws whose 1-norm condition estimate ||B||_1 ||B^-1||_1
+      (scipy's onenormest) exceeds it are repeated too (PDHG's iteration
+      count grows with that condition number).
+
+    Then c = A^T y0 + s0 and x0, y0 are the unique optimal pair with strict
+    complementarity.  ``meta`` holds x0, y0 and the boolean masks.
+    """
+    import scipy.sparse.linalg as spla
+
+    rng = np.random.default_rng(seed)
+    k = np.full(n, nnz_per_col, dtype=np.int64)
+    n_eq = int(round(m * eq_frac))
+    for _ in range(100):
+        rows, cols = _distinct_rows(rng, n, m, k)
+        vals = rng.standard_normal(rows.shape[0])
+        A = sp.csr_matrix((vals, (rows, cols)), shape=(m, n))
+        A.sum_duplicates()
+        A.sort_indices()
+        tight = np.ones(m, dtype=bool)
+        tight[n_eq:] = rng.random(m - n_eq) < tight_frac
+        r = int(tight.sum())
+        if r > n:
+            raise ValueError("more tight rows than columns")
+        interior = np.zeros(n, dtype=bool)
+        interior[rng.choice(n, r, replace=False)] = True
+        B = A[np.flatnonzero(tight)][:, np.flatnonzero(interior)].tocsc()
+        try:
+            lu = spla.splu(B)
+        except RuntimeError:
+            continue
+        if max_cond is not None:
+            inv = spla.LinearOperator(B.shape, matvec=lu.solve, rmatvec=lambda v: lu.solve(v, trans="T"),
+                                      dtype=np.float64)
+            if spla.onenormest(inv) * spla.norm(B, 1) > max_cond:
+                continue
+        break
+    else:
+        raise RuntimeError("no nonsingular basis found")
+    x0 = np.where(interior, rng.uniform(0.1 * ub, 0.9 * ub, size=n), 0.0)
+    upper = ~interior & (rng.random(n) < 0.5)
+    x0[upper] = ub
+    y0 = rng.standard_normal(m)
+    y0[n_eq:] = -np.abs(y0[n_eq:]) - 0.1
+    y0[~tight] = 0.0
+    s0 = rng.uniform(0.1, 1.0, size=n)
+    s0[interior] = 0.0
+    s0[upper] *= -1.0
+    c = A.T @ y0 + s0
+    b = A @ x0
+    hi = b.copy()
+    hi[~tight] += rng.uniform(0.1, 1.0, size=int((~tight).sum()))
+    lo = np.where(np.arange(m) < n_eq, b, -np.inf)
+    return LP(Csr.from_scipy(A), c, np.zeros(n), np.full(n, ub), lo, hi, name=name or f"nondeg_m{m}_n{n}_s{seed}",
+              meta={"x0": x0, "y0": y0, "interior": interior, "tight": tight})
+
+
+def diff_batch(count: int = 256, m: int = 500, n: int = 1000, nnz_per_col: int = 10, seed: int = 2000,
+               max_cond: float | None = 5e4) -> list:
+    """Batch of the differentiable-layer workload: ``count`` nondegenerate LPs
+    of one shape, seeds ``seed + i``, basis 1-norm condition estimate <=
+    ``max_cond``."""
+    return [nondegenerate_lp(m, n, nnz_per_col, seed=seed + i, max_cond=max_cond) for i in range(count)]
 
 
 def infeasible_lp(m: int = 200, n: int = 500, seed: int = 3) -> LP:

@@ -257,23 +257,62 @@ int gb_batch_schedule(gb_batch* b, int* threads, int* blocks_per_sm, int* groups
 void gb_batch_destroy(gb_batch* b);
 
 /* ---------------------------------------------------------------- 3b. differentiable solving
- * Forward: restarted PDHG to opt->tol on every instance of a batch, then
- * `tail_iters` (K) plain PDHG iterations in FP64 with fixed steps, storing a
- * checkpoint of (x, y) every `ckpt_every` (R) iterations; the outputs are the
- * last tail iterate (x*, y*) in original units.
- * Backward: given dL/dx* and dL/dy*, reverse-mode through the K tail
- * iterations (recomputing each R-segment from its checkpoint) and the
- * scaling, returning dL/dc, dL/dlo, dL/dhi and dL/d(A values) (CSR order of
- * the input A) in original units. */
+ * No counterpart in the reference (it differentiates run_pdhg,
+ * src/pdhg_impl.hpp:243-328).  LPs only.
+ * Forward: the batch engine solves every instance to opt->tol, then
+ * `tail_iters` (K) plain PDHG iterations run in FP64 with the final step
+ * sizes and no restart, keeping a checkpoint of (x, y) every `ckpt_every` (R)
+ * iterations; the outputs are the last tail iterate (x*, y*) in original
+ * units, certified again in FP64 (results[] report that point's KKT).
+ * Unless switched off, the tail starts from a POLISHED point: the active set
+ * one PDHG step reads off the solver's point defines a reduced KKT system
+ * (B^T y_D = c_F, B x_F = b_D - A[D,N] x_N, B = A[D,F]), solved per instance by
+ * MINRES; the vertex it gives replaces the PDHG point when it certifies
+ * better in FP64 (OSQP-style polishing).  A polished start is a fixed point of
+ * the PDHG map, so the tail then reproduces it.
+ * Backward: given dL/dx* and dL/dy*, exact reverse mode through the K tail
+ * iterations (each R-segment recomputed from its checkpoint; projections,
+ * extrapolation and the scaling are differentiated), then -- unless switched
+ * off -- an implicit completion that accounts for the tail start being a
+ * fixed point of the PDHG map: a per-instance MINRES solve on the projection
+ * masks of that point (for a nondegenerate vertex this is the basis
+ * sensitivity).  Returns dL/dc, dL/dlo, dL/dhi and dL/d(A values) (CSR order
+ * of the input A) in original units; scaling factors are held constant. */
 typedef struct gb_diff gb_diff;
+typedef struct {
+    int64_t implicit_max_iters;     /* MINRES steps per instance at most (0: truncated gradient,
+                                       the exact gradient of the K-step map with its start held fixed);
+                                       also bounds the polishing solve */
+    double implicit_tol;            /* relative residual at which MINRES stops */
+    int32_t polish;                 /* polish the solver's point before the tail */
+    int32_t pad;
+} gb_diff_options;
+void gb_diff_default_options(gb_diff_options* o); /* 20000, 1e-10, polish on */
+typedef struct {
+    double tau, sigma;              /* tail step sizes (scaled problem) */
+    int64_t tail_iterations;        /* K */
+    int64_t checkpoint_every;       /* R */
+    int64_t implicit_iterations;    /* MINRES steps of the last backward */
+    double implicit_residual;       /* its final relative residual */
+    int32_t implicit_converged;     /* residual <= implicit_tol reached */
+    int32_t free_cols;              /* columns strictly inside their box at the tail start (-1: unknown) */
+    int32_t active_rows;            /* rows whose dual is not projected to 0 there (-1: unknown) */
+    int32_t polished;               /* the tail started from the polished vertex */
+    int64_t polish_iterations;      /* MINRES steps of the polishing solve */
+    int64_t launches;               /* kernel launches of the last forward / backward call */
+} gb_diff_info;
 int gb_diff_create(int count, const gb_lp* lps, const gb_options* opt, int tail_iters, int ckpt_every,
                    gb_diff** out);
+int gb_diff_set_options(gb_diff* d, const gb_diff_options* o);
 /* x_out: concatenation of the instances' x (sum n), y_out: of y (sum m). */
 int gb_diff_forward(gb_diff* d, const gb_options* opt, gb_result* results, double* x_out, double* y_out);
-/* dl_dx (sum n), dl_dy (sum m) in; dl_dc (sum n), dl_dlo / dl_dhi (sum m),
- * dl_dval (sum nnz) out.  Any output may be NULL. */
+/* dl_dx (sum n), dl_dy (sum m) in (NULL = zero); dl_dc (sum n), dl_dlo /
+ * dl_dhi (sum m), dl_dval (sum nnz) out.  Any output may be NULL. */
 int gb_diff_backward(gb_diff* d, const double* dl_dx, const double* dl_dy, double* dl_dc, double* dl_dlo,
                      double* dl_dhi, double* dl_dval);
+int gb_diff_get_info(gb_diff* d, int i, gb_diff_info* out);
+/* Scaled tail start point z_0 (sum n, sum m), for checking the K-step map. */
+int gb_diff_tail_start(gb_diff* d, double* x_scaled, double* y_scaled);
 void gb_diff_destroy(gb_diff* d);
 
 #ifdef __cplusplus

@@ -68,3 +68,20 @@ def test_no_device_error_is_reported_not_thrown(lib):
     with pytest.raises(GanitError) as e:
         solve_pdhg_gpu(workloads.random_feasible_lp(20, 40, 3, seed=1))
     assert e.value.code in (-2, -4)
+
+
+def test_diff_argument_checks_without_gpu(lib):
+    """gb_diff_create validates K, R and the no-Hessian rule before touching a device."""
+    import numpy as np
+
+    from ganit_v2_b200 import GanitError, workloads as W
+    from ganit_v2_b200.api import DiffSolver
+
+    lp = W.random_feasible_lp(20, 40, 3, seed=1)
+    with pytest.raises(GanitError, match="multiple of ckpt_every"):
+        DiffSolver([lp], tail_iters=30, ckpt_every=20)
+    with pytest.raises(GanitError, match="multiple of ckpt_every"):
+        DiffSolver([lp], tail_iters=0, ckpt_every=1)
+    qp = W.portfolio_qp(200, 3, seed=1)
+    with pytest.raises(GanitError, match="LPs only"):
+        DiffSolver([qp], tail_iters=20, ckpt_every=10)

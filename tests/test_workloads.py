@@ -59,3 +59,37 @@ def test_infeasible_lp_has_contradicting_rows():
     r1, r2 = A.getrow(lp.m - 2).toarray(), A.getrow(lp.m - 1).toarray()
     assert np.array_equal(r1, r2)
     assert lp.hi[-2] < lp.lo[-1]
+
+
+def test_nondegenerate_lp_has_a_strictly_complementary_unique_vertex():
+    lp = W.nondegenerate_lp(80, 200, 6, seed=3)
+    A = lp.A.to_scipy().tocsr()
+    x0, y0, interior, tight = (lp.meta[k] for k in ("x0", "y0", "interior", "tight"))
+    ax = A @ x0
+    # primal feasibility; tight rows hold with equality, the others with slack >= 0.1
+    assert np.all(x0 >= lp.l) and np.all(x0 <= lp.u)
+    assert np.allclose(ax[tight], lp.hi[tight], atol=1e-9)
+    assert np.all(lp.hi[~tight] - ax[~tight] >= 0.1 - 1e-12)
+    eq = np.isfinite(lp.lo)
+    assert np.allclose(ax[eq], lp.lo[eq], atol=1e-9)
+    # dual: y <= -0.1 on tight <= rows, 0 on slack rows; reduced costs strictly signed at bounds
+    assert np.all(y0[~eq & tight] <= -0.1) and np.all(y0[~tight] == 0.0)
+    d = lp.c - A.T @ y0
+    assert np.allclose(d[interior], 0.0, atol=1e-9)
+    at_l = ~interior & (x0 == 0.0)
+    at_u = ~interior & (x0 == 10.0)
+    assert np.all(d[at_l] >= 0.1 - 1e-9) and np.all(d[at_u] <= -0.1 + 1e-9)
+    # square nonsingular basis
+    B = A[np.flatnonzero(tight)][:, np.flatnonzero(interior)].toarray()
+    assert B.shape[0] == B.shape[1] and np.linalg.matrix_rank(B) == B.shape[0]
+
+
+def test_diff_batch_is_deterministic_and_conditioned():
+    a = W.diff_batch(3, 50, 100, 5, seed=10, max_cond=1e4)
+    b = W.diff_batch(3, 50, 100, 5, seed=10, max_cond=1e4)
+    for x, y in zip(a, b):
+        assert np.array_equal(x.A.val, y.A.val) and np.array_equal(x.c, y.c)
+    for lp in a:
+        A = lp.A.to_scipy().tocsr()
+        B = A[np.flatnonzero(lp.meta["tight"])][:, np.flatnonzero(lp.meta["interior"])].toarray()
+        assert np.linalg.cond(B, 1) <= 1e4 * 1.0001
