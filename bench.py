@@ -16,6 +16,10 @@ download of x and y all inside the timed region.
 
 Multi-GPU (torchrun): a single LP does not shard, so every rank solves its
 own replica (weak scaling); value = all ranks' solves / max-over-ranks time.
+The batched workloads reported alongside (``batch``: 512 random LPs;
+``diff``: the differentiable layer on 256 LPs) split their instances over the
+ranks by the nnz-balanced partition of ganit_v2_b200.shard (no exchange;
+time = max over ranks).
 
 ``--impl reference`` times the reference's own CPU implementation
 (ganit::solve_pdhg_cpu, oracle/_ref/libganit_ref.so built from the reference
@@ -202,55 +206,232 @@ def run_profile_case():
     return 0
 
 
-def batch_measure(steps: int = 3, seq_sample: int = 24) -> dict:
+def reduce_sum(dist, v: float) -> float:
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def run_profile_batch():
+    """The 512-LP batch shortened for ncu: one mixed solve (launch it with
+    GANIT_B200_LAUNCH=stream so no conditional graph is involved), then 3
+    plain FP32 iterations with every instance active."""
+    import ganit_v2_b200 as gb
+    from ganit_v2_b200 import workloads as W
+
+    gb.set_device(0)
+    lps = W.lp_batch(512, seed=1000)
+    opt = gb.Options(precision=gb.Precision.Mixed)
+    with gb.BatchSolver(lps, opt) as bs:
+        res = bs.solve(opt, fetch=False)
+        k = bs.time_kernels(0, 3)
+    print(json.dumps({"profile_case": "512-LP batch", "optimal": sum(r.status_name == "OPTIMAL" for r in res),
+                      "bytes_per_iter_f32": k["bytes_per_iter"]}))
+    return 0
+
+
+def batch_measure(dist, rank: int, world: int, steps: int = 3, seq_sample: int = 24) -> dict:
     """512 random feasible LPs of log-uniform size (m in [50, 4000],
     n = 2.5 m, 4-12 nonzeros per column, seeds 1000..1511): LPs/s of the
     batched mixed-precision solver (every result FP64-certified) against the
     plain FP64 single-instance path on the same GPU, looping over the first
-    `seq_sample` instances one by one (each resident beforehand)."""
+    `seq_sample` instances one by one (each resident beforehand).  Row-split
+    schedules come from the autotuner.  With N ranks the instances are split
+    by the nnz-balanced partition (no exchange; time = max over ranks)."""
+    import torch
+
     import ganit_v2_b200 as gb
-    from ganit_v2_b200 import workloads as W
+    from ganit_v2_b200 import shard, workloads as W
 
     lps = W.lp_batch(512, seed=1000)
+    part = shard.partition([shard.instance_weight(lp) for lp in lps], world)[rank]
+    mine = [lps[i] for i in part]
     mixed = gb.Options(precision=gb.Precision.Mixed)
     fp64 = gb.Options(precision=gb.Precision.Double)
     t0 = time.perf_counter()
-    bs = gb.BatchSolver(lps, mixed)
+    bs = gb.BatchSolver(mine, mixed)
     setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tune = bs.autotune(iters=30)
+    tune_s = time.perf_counter() - t0
     res = bs.solve(mixed, fetch=False)
     secs = []
     for _ in range(steps):
+        torch.cuda.synchronize()
+        barrier(dist)
         t0 = time.perf_counter()
         res = bs.solve(mixed, fetch=False)
         secs.append(time.perf_counter() - t0)
+    t_batch = reduce_max(dist, min(secs))
+    kt = bs.time_kernels(0, 50)
+    kt64 = bs.time_kernels(2, 20)
     sched = bs.schedule()
     bs.close()
-    n_opt = sum(r.status == gb.Status.Optimal for r in res)
-    certified = sum(r.status == gb.Status.Optimal and max(r.rel_primal, r.rel_dual, r.rel_gap) <= 1e-4 * 1.0000001
-                    for r in res)
-    probs = [gb.Problem(lp, fp64) for lp in lps[:seq_sample]]
-    for p in probs[:2]:
-        p.solve(fp64, fetch=False)
-    t0 = time.perf_counter()
-    for p in probs:
-        p.solve(fp64, fetch=False)
-    seq_s = time.perf_counter() - t0
-    for p in probs:
-        p.close()
-    batch_lps = len(lps) / min(secs)
-    seq_lps = seq_sample / seq_s
+    n_opt = reduce_sum(dist, sum(r.status == gb.Status.Optimal for r in res))
+    certified = reduce_sum(dist, sum(r.status == gb.Status.Optimal and
+                                     max(r.rel_primal, r.rel_dual, r.rel_gap) <= 1e-4 * 1.0000001 for r in res))
+    it_max = reduce_max(dist, max(r.iterations for r in res))
+    seq_lps = None
+    if rank == 0:
+        probs = [gb.Problem(lp, fp64) for lp in lps[:seq_sample]]
+        for p in probs[:2]:
+            p.solve(fp64, fetch=False)
+        t0 = time.perf_counter()
+        for p in probs:
+            p.solve(fp64, fetch=False)
+        seq_lps = seq_sample / (time.perf_counter() - t0)
+        for p in probs:
+            p.close()
+    peak, peak_kind = measured_peaks()
+    it_ms = kt["ms_primal"] + kt["ms_dual"]
+    gbs = kt["bytes_per_iter"] / (it_ms / 1e3) / 1e9
+    gbs64 = kt64["bytes_per_iter"] / ((kt64["ms_primal"] + kt64["ms_dual"]) / 1e3) / 1e9
+    batch_lps = len(lps) / t_batch
+    bn = tune["block_nnz"]
+    mr = tune["max_rows"]
     return {"workload": "512 random feasible LPs, m log-uniform [50,4000], n=2.5m, 4-12 nnz/col "
                         f"(sum nnz {sum(lp.A.nnz for lp in lps)})",
-            "lps_per_s": batch_lps, "ms_per_batch": 1e3 * min(secs), "setup_s": setup_s,
-            "optimal": n_opt, "certified_1e-4": certified, "iterations_max": max(r.iterations for r in res),
-            "iterations_mean": float(np.mean([r.iterations for r in res])),
+            "lps_per_s": batch_lps, "ms_per_batch": 1e3 * t_batch, "setup_s": setup_s,
+            "parallelism": f"instances split over {world} GPUs (nnz-balanced)" if world > 1 else "single GPU",
+            "optimal": int(n_opt), "certified_1e-4": int(certified), "iterations_max": int(it_max),
+            "iterations_mean_rank0": float(np.mean([r.iterations for r in res])),
             "fp64_single_instance_loop_lps_per_s": seq_lps,
             "fp64_loop_sample": f"first {seq_sample} instances solved one by one (FP64, resident)",
-            "speedup_vs_fp64_loop": batch_lps / seq_lps,
+            "speedup_vs_fp64_loop": (batch_lps / seq_lps) if seq_lps else None,
+            "iteration_kernels": {"bound": "hbm", "ms_primal_f32": kt["ms_primal"], "ms_dual_f32": kt["ms_dual"],
+                                  "ms_per_iter_f32": it_ms, "bytes_per_iter_f32": kt["bytes_per_iter"],
+                                  "gbs_f32": gbs, "frac_f32": gbs / peak,
+                                  "ms_per_iter_f64": kt64["ms_primal"] + kt64["ms_dual"], "gbs_f64": gbs64,
+                                  "frac_f64": gbs64 / peak, "peak": peak, "peak_source": f"{peak_kind} hbm_gbs",
+                                  "note": "k_primal + k_dual over all instances (rank 0's shard), CUDA events, "
+                                          "every instance active; bytes = 2 nnz (s_M+4) + 4 (m+n+2) + s_V (9n+7m)"},
+            "autotune": {"seconds": tune_s, "ms_per_iter_default": tune["ms_per_iter_default"],
+                         "ms_per_iter_tuned": tune["ms_per_iter_tuned"],
+                         "choices": {f"{b}x{r}": int(np.sum((bn == b) & (mr == r)))
+                                     for b, r in sorted(set(zip(bn.tolist(), mr.tolist())))}},
             "schedule": {"threads": sched["threads"], "blocks_per_sm": sched["blocks_per_sm"],
                          "group_A_hist": np.bincount(np.log2(sched["groups_A"]).astype(int), minlength=6).tolist(),
                          "group_AT_hist": np.bincount(np.log2(sched["groups_AT"]).astype(int), minlength=6).tolist()},
-            "timing": "host wall clock around gb_batch_solve (synchronous), best of %d" % steps}
+            "timing": "host wall clock around gb_batch_solve (synchronous), best of %d, max over ranks" % steps}
+
+
+def diff_measure(dist, rank: int, world: int, count: int = 256, steps: int = 2, check: int = 2) -> dict:
+    """Differentiable batched LP layer: `count` nondegenerate LPs of m=500,
+    n=1000, 10 nnz/col (the random-LP family with a unique strictly
+    complementary optimum; workloads.diff_batch), forward = mixed-precision
+    restarted PDHG to 1e-6 + polishing + K=200 tail iterations checkpointed
+    every R=20, backward = reverse pass + implicit completion for
+    L = w.x* + v.y*.  Gradients of `check` instances are compared with the
+    basis sensitivities of the reference dual simplex (and one central
+    difference, h=1e-4, of its exact solution map)."""
+    import torch
+
+    import ganit_v2_b200 as gb
+    from ganit_v2_b200 import shard, workloads as W
+
+    lps = W.diff_batch(count)
+    part = shard.partition([shard.instance_weight(lp) for lp in lps], world)[rank]
+    mine = [lps[i] for i in part]
+    opt = gb.Options(tol=1e-6, precision=gb.Precision.Mixed)
+    t0 = time.perf_counter()
+    ds = gb.DiffSolver(mine, opt, tail_iters=200, ckpt_every=20)
+    setup_s = time.perf_counter() - t0
+    rng = np.random.default_rng(3)
+    w = rng.standard_normal(int(ds.n_off[-1]))
+    v = rng.standard_normal(int(ds.m_off[-1]))
+    res, x, y = ds.forward(opt)
+    g = ds.backward(w, v)
+    tf, tb = [], []
+    launches_f = launches_b = 0
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        barrier(dist)
+        t0 = time.perf_counter()
+        res, x, y = ds.forward(opt)
+        tf.append(time.perf_counter() - t0)
+        launches_f = ds.info(0)["launches"]
+        torch.cuda.synchronize()
+        barrier(dist)
+        t0 = time.perf_counter()
+        g = ds.backward(w, v)
+        tb.append(time.perf_counter() - t0)
+        launches_b = ds.info(0)["launches"]
+    t_f = reduce_max(dist, min(tf))
+    t_b = reduce_max(dist, min(tb))
+    infos = [ds.info(i) for i in range(len(mine))]
+    opt_n = reduce_sum(dist, sum(r.status == gb.Status.Optimal for r in res))
+    pol = reduce_sum(dist, sum(i["polished"] for i in infos))
+    conv = reduce_sum(dist, sum(i["implicit_converged"] for i in infos))
+    mr_max = reduce_max(dist, max(i["implicit_iterations"] for i in infos))
+    its_max = reduce_max(dist, max(r.iterations for r in res))
+    errs, fd_err = [], None
+    if rank == 0:
+        from oracle import oracle as O
+
+        n0 = ds.n_off
+        m0 = ds.m_off
+        z0 = ds.nnz_off
+        for i in range(min(check, len(mine))):
+            lp = mine[i]
+            A = lp.A.to_scipy().tocsr()
+            if O.ref_available():
+                sx = O.ref_dual_simplex(lp)
+                head = sx["head"]
+                basic = np.sort(head[head < lp.n])
+                act = np.ones(lp.m, dtype=bool)
+                act[head[head >= lp.n] - lp.n] = False
+                X, Y = sx["x"], sx["y"]
+            else:
+                basic, act = np.flatnonzero(lp.meta["interior"]), lp.meta["tight"]
+                X, Y = lp.meta["x0"], lp.meta["y0"]
+            B = A[np.flatnonzero(act)][:, basic].toarray()
+            wi, vi = w[n0[i]:n0[i + 1]], v[m0[i]:m0[i + 1]]
+            p = np.zeros(lp.m)
+            q = np.zeros(lp.n)
+            p[act] = np.linalg.solve(B.T, wi[basic])
+            q[basic] = np.linalg.solve(B, vi[act])
+            rows = np.repeat(np.arange(lp.m), np.diff(lp.A.ptr))
+            da = -(p[rows] * X[lp.A.idx] + Y[rows] * q[lp.A.idx])
+            rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
+            errs.append([rel(g["c"][n0[i]:n0[i + 1]], q), rel(g["lo"][m0[i]:m0[i + 1]] + g["hi"][m0[i]:m0[i + 1]], p),
+                         rel(g["a_val"][z0[i]:z0[i + 1]], da)])
+        if O.ref_available() and mine:
+            from ganit_v2_b200.lp import LP, Csr
+
+            lp = mine[0]
+            d = np.random.default_rng(5)
+            dc, db, da_ = d.standard_normal(lp.n), d.standard_normal(lp.m), d.standard_normal(lp.A.nnz)
+            h = 1e-4
+
+            def lval(sgn):
+                lo = np.where(np.isfinite(lp.lo), lp.lo + sgn * h * db, lp.lo)
+                hi = lp.hi + sgn * h * db
+                r = O.ref_dual_simplex(LP(Csr(lp.m, lp.n, lp.A.ptr, lp.A.idx, lp.A.val + sgn * h * da_),
+                                          lp.c + sgn * h * dc, lp.l, lp.u, lo, hi))
+                return w[:lp.n] @ r["x"] + v[:lp.m] @ r["y"]
+
+            fd = (lval(1.0) - lval(-1.0)) / (2 * h)
+            an = (g["c"][:lp.n] @ dc + (g["lo"][:lp.m] * np.isfinite(lp.lo)) @ db + g["hi"][:lp.m] @ db +
+                  g["a_val"][:lp.A.nnz] @ da_)
+            fd_err = abs(an - fd) / abs(fd)
+    return {"workload": f"{count} nondegenerate LPs m=500 n=1000 10 nnz/col (sum nnz {sum(lp.A.nnz for lp in lps)})",
+            "lps_per_s_forward_backward": count / (t_f + t_b), "forward_ms": 1e3 * t_f, "backward_ms": 1e3 * t_b,
+            "setup_s": setup_s, "tail_iters": 200, "ckpt_every": 20,
+            "optimal_1e-6": int(opt_n), "polished": int(pol), "implicit_converged": int(conv),
+            "implicit_minres_iters_max": int(mr_max), "pdhg_iterations_max": int(its_max),
+            "forward_launches": launches_f, "backward_launches": launches_b,
+            "grad_rel_err_vs_dual_simplex_basis": {"instances": len(errs),
+                                                   "max_c": max((e[0] for e in errs), default=None),
+                                                   "max_b": max((e[1] for e in errs), default=None),
+                                                   "max_A": max((e[2] for e in errs), default=None)},
+            "grad_rel_err_vs_central_fd_h1e-4": fd_err,
+            "parallelism": f"instances split over {world} GPUs (nnz-balanced)" if world > 1 else "single GPU",
+            "timing": f"host wall clock around gb_diff_forward / gb_diff_backward (synchronous), best of {steps}, "
+                      "max over ranks"}
 
 
 def pinned_copy(lp):
@@ -279,13 +460,17 @@ def main():
     ap.add_argument("--kernel-iters", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-LP batch measurement")
-    ap.add_argument("--profile", action="store_true",
-                    help="short fixed sequence for ncu: upload + one warm-up solve + one solve + 3 timed iterations")
+    ap.add_argument("--no-diff", action="store_true", help="skip the differentiable-layer measurement")
+    ap.add_argument("--profile", nargs="?", const="single", choices=["single", "batch"],
+                    help="short fixed sequence for ncu: 'single' = the blending LP (upload, two solves, 3 timed "
+                         "iterations per level); 'batch' = the 512-LP batch (one solve, 3 timed FP32 iterations)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.profile == "batch":
+        return run_profile_batch()
     if args.profile:
         return run_profile_case()
 
@@ -373,7 +558,10 @@ def main():
 
     batch = None
     if not args.no_batch:
-        batch = batch_measure()
+        batch = batch_measure(dist, rank, world)
+    diff = None
+    if not args.no_diff:
+        diff = diff_measure(dist, rank, world)
     line = None
     if rank == 0:
         cpu = None
@@ -412,6 +600,7 @@ def main():
             "clocks": clk,
             "cpu_baseline": cpu,
             "batch": batch,
+            "diff": diff,
         }
         print(json.dumps(line), flush=True)
     prob.close()

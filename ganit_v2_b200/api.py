@@ -153,7 +153,8 @@ EXPORTS = [
     "gb_vec_from_host", "gb_vec_to_host", "gb_vec_size", "gb_vec_destroy", "gb_copy", "gb_fill", "gb_spmv_A",
     "gb_spmv_AT", "gb_spmv_Q", "gb_primal_step", "gb_dual_step", "gb_sub", "gb_scale_into", "gb_primal_res2",
     "gb_dual_res", "gb_row_dual_obj", "gb_dot", "gb_dot_c", "gb_diff2", "gb_batch_create", "gb_batch_solve",
-    "gb_batch_get_solution", "gb_batch_schedule", "gb_batch_destroy", "gb_diff_create", "gb_diff_forward",
+    "gb_batch_get_solution", "gb_batch_schedule", "gb_batch_autotune", "gb_batch_time_kernels", "gb_batch_destroy",
+    "gb_diff_create", "gb_diff_forward",
     "gb_diff_default_options", "gb_diff_set_options", "gb_diff_backward", "gb_diff_get_info", "gb_diff_tail_start", "gb_diff_destroy",
     "gb_eval_kkt_noalloc",
 ]
@@ -188,6 +189,8 @@ def load_library(path: str = LIB_PATH):
         "gb_dot": (i32, [vp, vp, vp, vp]), "gb_dot_c": (i32, [vp, vp, vp]), "gb_diff2": (i32, [vp, vp, vp, vp]),
         "gb_batch_create": (i32, [i32, vp, vp, vp]), "gb_batch_solve": (i32, [vp, vp, vp]),
         "gb_batch_get_solution": (i32, [vp, i32, vp, vp]), "gb_batch_schedule": (i32, [vp, vp, vp, vp]),
+        "gb_batch_autotune": (i32, [vp, i32, vp, vp, vp, vp]),
+        "gb_batch_time_kernels": (i32, [vp, i32, i32, vp, vp, vp, vp]),
         "gb_batch_destroy": (None, [vp]), "gb_diff_create": (i32, [i32, vp, vp, i32, i32, vp]),
         "gb_diff_forward": (i32, [vp, vp, vp, vp, vp]), "gb_diff_default_options": (None, [vp]),
         "gb_diff_set_options": (i32, [vp, vp]),
@@ -382,6 +385,23 @@ class BatchSolver:
         g = np.zeros(2 * len(self.lps), dtype=np.int32)
         _check(self._lib.gb_batch_schedule(self._h, C.byref(t), C.byref(b), _p(g)))
         return {"threads": t.value, "blocks_per_sm": b.value, "groups_A": g[0::2].copy(), "groups_AT": g[1::2].copy()}
+
+    def autotune(self, iters: int = 30) -> dict:
+        """Pick row-split schedules per instance-size class by timing (gb_batch_autotune)."""
+        k = len(self.lps)
+        bn = np.zeros(k, dtype=np.int32)
+        mr = np.zeros(k, dtype=np.int32)
+        t0, t1 = C.c_double(), C.c_double()
+        _check(self._lib.gb_batch_autotune(self._h, int(iters), _p(bn), _p(mr), C.byref(t0), C.byref(t1)))
+        return {"block_nnz": bn, "max_rows": mr, "ms_per_iter_default": t0.value, "ms_per_iter_tuned": t1.value}
+
+    def time_kernels(self, level: int = 0, iters: int = 50) -> dict:
+        """Device time of the fused iteration kernels with every instance active."""
+        mp, md, bpi = C.c_double(), C.c_double(), C.c_double()
+        nl = C.c_int64()
+        _check(self._lib.gb_batch_time_kernels(self._h, int(level), int(iters), C.byref(mp), C.byref(md),
+                                               C.byref(nl), C.byref(bpi)))
+        return {"ms_primal": mp.value, "ms_dual": md.value, "launches": nl.value, "bytes_per_iter": bpi.value}
 
     def close(self):
         if getattr(self, "_h", None):

@@ -315,6 +315,8 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     GB_CUDA(cudaMemsetAsync(P->arrive.get(), 0, sizeof(unsigned), s));
 
     // schedules (host, from the row-length histogram, per instance) and transpose
+    P->tune_block_nnz.assign(count, kBlockNnz);
+    P->tune_max_rows.assign(count, kThreads);
     P->A.sched.upload(build_schedule(P->A.host_ptr.data(), m, P->row_off.data(), count), 3, s);
     device_transpose(*P, s);
     P->AT.sched.upload(build_schedule(P->AT.host_ptr.data(), n, P->col_off.data(), count), 3, s);
@@ -361,7 +363,7 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     P->dplr = P->has_q && L0.q_rank > 0;
     P->qk = P->dplr ? L0.q_rank : 0;
     P->partials.reset(std::max<size_t>(static_cast<size_t>(kFtxGrid) * 2 * kMaxRank,
-                                       static_cast<size_t>(P->A.sched.nb + P->AT.sched.nb) * kTerms));
+                                       static_cast<size_t>(P->A.sched.nb + P->AT.sched.nb + count) * kTerms));
     P->ftx.reset(2 * kMaxRank);
     P->v32.alloc(n, m, P->qk, P->has_q);
     P->v64.alloc(n, m, P->qk, P->has_q);
@@ -481,6 +483,7 @@ EvalArgs<M, V> eval_args(Problem& P, VecSet<V>& vs, const V* x, const V* y, int 
     a.st = P.st.get();
     a.arrive = P.arrive.get();
     a.partials = P.partials.get();
+    a.inst_terms = P.partials.get() + static_cast<size_t>(P.A.sched.nb + P.AT.sched.nb) * kTerms;
     a.cond = 0;
     a.use_cond = 0;
     return a;
@@ -837,6 +840,91 @@ void time_level(Problem& P, int iters, double* msp, double* msd, int64_t* launch
     *launches = nl;
 }
 
+// Rebuild both schedules from the per-instance tunables; captured graphs
+// hold the old schedule and are dropped.
+void rebuild_schedules(Problem& P) {
+    cudaStream_t s = P.stream;
+    GB_CUDA(cudaStreamSynchronize(s));
+    for (auto& g : P.graphs) g.reset();
+    P.A.sched.upload(build_schedule(P.A.host_ptr.data(), P.row_off.data(), P.count, P.tune_block_nnz.data(),
+                                    P.tune_max_rows.data()),
+                     3, s);
+    P.AT.sched.upload(build_schedule(P.AT.host_ptr.data(), P.col_off.data(), P.count, P.tune_block_nnz.data(),
+                                     P.tune_max_rows.data()),
+                      3, s);
+    const size_t need = static_cast<size_t>(P.A.sched.nb + P.AT.sched.nb + P.count) * kTerms;
+    if (P.partials.size() < need) P.partials.reset(need);
+    GB_CUDA(cudaStreamSynchronize(s));
+}
+
+// Row-split schedule autotuner.  Instances are binned into (at most) four
+// classes of equal total nonzeros by instance size; for each class in turn
+// every candidate (block_nnz, max_rows) -- block_nnz bounds the nonzeros a
+// STREAM block stages (<= kBlockNnz, the shared-memory product buffer),
+// max_rows the rows it reduces and hence the lanes per row -- is tried with
+// the other classes at their incumbents, by timing `iters` fused FP32
+// iterations (CUDA events around k_primal + k_dual), and kept when it is
+// more than 1% faster.  The per-row group size inside a block still follows
+// the block's row count (the row-length histogram).
+void autotune(Problem& P, int iters, double* ms_default, double* ms_tuned) {
+    static const int cand[][2] = {{2048, 256}, {2048, 128}, {2048, 64}, {1024, 256}, {1024, 128},
+                                  {1024, 64},  {1024, 32},  {512, 64},  {512, 32}};
+    auto measure = [&]() {
+        double best = INFINITY;
+        for (int rep = 0; rep < 2; ++rep) {
+            double mp = 0, md = 0;
+            int64_t nl = 0;
+            time_level<float, float>(P, iters, &mp, &md, &nl);
+            best = std::min(best, mp + md);
+        }
+        return best;
+    };
+    P.tune_block_nnz.assign(P.count, kBlockNnz);
+    P.tune_max_rows.assign(P.count, kThreads);
+    rebuild_schedules(P);
+    double best = measure();
+    if (ms_default) *ms_default = best;
+    // classes by instance size
+    std::vector<int> order(P.count);
+    std::iota(order.begin(), order.end(), 0);
+    auto nnz_of = [&](int k) { return static_cast<long long>(P.nnz_off[k + 1]) - P.nnz_off[k]; };
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return nnz_of(a) < nnz_of(b); });
+    const long long total = P.nnz_off[P.count];
+    const int nclass = std::min(4, P.count);
+    std::vector<std::vector<int>> cls(nclass);
+    long long acc = 0;
+    for (int k : order) {
+        const int c = std::min(nclass - 1, static_cast<int>(total ? (acc * nclass) / total : 0));
+        cls[c].push_back(k);
+        acc += nnz_of(k);
+    }
+    for (const auto& members : cls) {
+        if (members.empty()) continue;
+        const int inc_b = P.tune_block_nnz[members[0]], inc_r = P.tune_max_rows[members[0]];
+        int win_b = inc_b, win_r = inc_r;
+        for (const auto& c : cand) {
+            if (c[0] == inc_b && c[1] == inc_r) continue;
+            for (int k : members) {
+                P.tune_block_nnz[k] = c[0];
+                P.tune_max_rows[k] = c[1];
+            }
+            rebuild_schedules(P);
+            const double t = measure();
+            if (t < 0.99 * best) {
+                best = t;
+                win_b = c[0];
+                win_r = c[1];
+            }
+        }
+        for (int k : members) {
+            P.tune_block_nnz[k] = win_b;
+            P.tune_max_rows[k] = win_r;
+        }
+    }
+    rebuild_schedules(P);
+    if (ms_tuned) *ms_tuned = measure();
+}
+
 void problem_stats(const Problem& P, int64_t* launches, double* bpi) {
     if (launches) *launches = P.launches;
     if (bpi) {
@@ -1026,6 +1114,34 @@ int gb_batch_schedule(gb_batch* b, int* threads, int* blocks_per_sm, int* groups
                 groups[2 * k] = mode_g(ba, P.A.sched.host_seg_block[k], P.A.sched.host_seg_block[k + 1]);
                 groups[2 * k + 1] = mode_g(bt, P.AT.sched.host_seg_block[k], P.AT.sched.host_seg_block[k + 1]);
             }
+        }
+    });
+}
+
+int gb_batch_autotune(gb_batch* b, int iters, int* block_nnz, int* max_rows, double* ms_default, double* ms_tuned) {
+    return guarded([&] {
+        GB_REQUIRE(b != nullptr && iters > 0, "bad arguments");
+        Problem& P = *b->p;
+        autotune(P, iters, ms_default, ms_tuned);
+        for (int k = 0; k < P.count; ++k) {
+            if (block_nnz) block_nnz[k] = P.tune_block_nnz[k];
+            if (max_rows) max_rows[k] = P.tune_max_rows[k];
+        }
+    });
+}
+
+int gb_batch_time_kernels(gb_batch* b, int level, int iters, double* ms_primal, double* ms_dual, int64_t* launches,
+                          double* bytes_per_iter) {
+    return guarded([&] {
+        GB_REQUIRE(b && iters > 0 && level >= 0 && level <= 2, "bad arguments");
+        Problem& P = *b->p;
+        if (level == 0) time_level<float, float>(P, iters, ms_primal, ms_dual, launches);
+        else if (level == 1) time_level<float, double>(P, iters, ms_primal, ms_dual, launches);
+        else time_level<double, double>(P, iters, ms_primal, ms_dual, launches);
+        if (bytes_per_iter) {
+            double bpi[3];
+            problem_stats(P, nullptr, bpi);
+            *bytes_per_iter = bpi[level];
         }
     });
 }

@@ -34,7 +34,9 @@ constexpr size_t kOffPartials = kOffBlocks + sizeof(RowBlock) * GB_NOALLOC_MAX_B
 constexpr size_t kOffSlots = kOffPartials + sizeof(double) * kTerms * GB_NOALLOC_MAX_BLOCKS;
 constexpr size_t kOffCounters = kOffSlots + sizeof(double) * GB_NOALLOC_MAX_SLOTS;
 constexpr size_t kOffSeg = kOffCounters + sizeof(unsigned) * GB_NOALLOC_MAX_LONG_ROWS;  // 2 x int[2] + arrive
-constexpr size_t kOffEnd = kOffSeg + 64;
+constexpr size_t kOffTerms = kOffSeg + 64;  // the last CTA's per-instance sums (one instance)
+constexpr size_t kOffEnd = kOffTerms + sizeof(double) * kTerms;
+static_assert(kOffTerms % alignof(double) == 0, "term slot misaligned");
 static_assert(sizeof(SolveState) <= kOffBlocks, "state slot too small");
 static_assert(kOffEnd <= kNoAllocScratchBytes, "scratch layout exceeds the array");
 
@@ -134,6 +136,7 @@ extern "C" int gb_eval_kkt_noalloc(const gb_scaled_lp* dev, const int32_t* h_a_p
         a.arrive = arrive;
         a.st = st;
         a.partials = partials;
+        a.inst_terms = reinterpret_cast<double*>(base + kOffTerms);
         a.use_cond = 0;
         k_eval<double, double, 1, 1><<<nb, kThreads, spmv_smem_bytes<1, double>(), s>>>(a);
         GB_CUDA(cudaGetLastError());

@@ -201,6 +201,7 @@ struct EvalArgs {
     SolveState* st;              // per instance
     unsigned* arrive;            // CTA arrival counter (re-armed by the last CTA)
     double* partials;            // [gridDim.x][kTerms]
+    double* inst_terms;          // [count][kTerms] scratch of the last CTA
     unsigned long long cond;     // cudaGraphConditionalHandle of the phase loop
     int use_cond;                // 1 inside the loop body: the decision drives the loop
 };
@@ -469,7 +470,9 @@ __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalA
     if (!am_last) return;
     // Last CTA: reduce every instance's partials in a fixed order and run its
     // decision.  An instance with many blocks is reduced by the whole CTA
-    // (one at a time), the others by one warp each.
+    // (one at a time); the others by one warp each into inst_terms, after
+    // which every thread runs the decisions of its own instances (the scalar
+    // decision code is the long part, so it must not run one instance per warp).
     __threadfence();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int any_active = 0;
@@ -506,17 +509,29 @@ __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalA
     }
     for (int k = wid; k < a.count; k += kWarps) {
         const int nblk = (a.seg_a[k + 1] - a.seg_a[k]) + (a.seg_t[k + 1] - a.seg_t[k]);
-        if (nblk > kWide) continue;
-        SolveState& s = a.st[k];
-        if (!eval_includes(s, a.mode)) {
-            if (lane == 0) s.ran_body = 0;
-            continue;
-        }
+        if (nblk > kWide || !eval_includes(a.st[k], a.mode)) continue;
         double T[kTerms];
         load_terms(k, lane, 32, T);
 #pragma unroll
         for (int q = 0; q < kTerms; ++q) T[q] = warp_sum(T[q]);
-        if (lane == 0) finish(s, T);
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < kTerms; ++q) a.inst_terms[static_cast<size_t>(k) * kTerms + q] = T[q];
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < a.count; k += kThreads) {
+        const int nblk = (a.seg_a[k + 1] - a.seg_a[k]) + (a.seg_t[k + 1] - a.seg_t[k]);
+        if (nblk > kWide) continue;
+        SolveState& s = a.st[k];
+        if (!eval_includes(s, a.mode)) {
+            s.ran_body = 0;
+            continue;
+        }
+        double T[kTerms];
+#pragma unroll
+        for (int q = 0; q < kTerms; ++q) T[q] = a.inst_terms[static_cast<size_t>(k) * kTerms + q];
+        finish(s, T);
     }
     any_active = __syncthreads_or(any_active);
     if (threadIdx.x == 0) {

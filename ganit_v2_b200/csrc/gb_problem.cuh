@@ -114,6 +114,8 @@ struct Problem {
     long long launches = 0;               // kernel launches of the last solve
     std::vector<InstanceResult> results;
     bool solved = false;
+    // row-split schedule tunables per instance (the batch autotuner sets them)
+    std::vector<int> tune_block_nnz, tune_max_rows;
 
     const int* icol() const { return count > 1 ? inst_col.get() : nullptr; }
     const int* irow() const { return count > 1 ? inst_row.get() : nullptr; }

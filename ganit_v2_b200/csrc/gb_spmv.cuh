@@ -121,6 +121,23 @@ inline Schedule build_schedule(const int* ptr, int rows, const int* seg_off = nu
     return s;
 }
 
+// Same with per-instance tunables (block_nnz <= kBlockNnz, max_rows <= kThreads).
+inline Schedule build_schedule(const int* ptr, const int* seg_off, int nseg, const int* block_nnz,
+                               const int* max_rows) {
+    Schedule s;
+    s.seg_block.assign(nseg + 1, 0);
+    for (int k = 0; k < nseg; ++k) {
+        s.seg_block[k] = static_cast<int>(s.blocks.size());
+        schedule_rows(ptr, seg_off[k], seg_off[k + 1], block_nnz[k], max_rows[k], &s.nslots, &s.ncounters, k,
+                      [&](const RowBlock& b) {
+                          s.blocks.push_back(b);
+                          s.max_lg = std::max(s.max_lg, b.lg);
+                      });
+    }
+    s.seg_block[nseg] = static_cast<int>(s.blocks.size());
+    return s;
+}
+
 // Device-resident schedule of one matrix.
 struct DevSchedule {
     DevBuf<RowBlock> blocks;

@@ -237,13 +237,14 @@ int gb_eval_kkt_noalloc(const gb_scaled_lp* dev, const int32_t* h_a_ptr, const i
                         const double* y, const gb_kkt_scalars* sc, void* stream, gb_kkt* out);
 
 /* ---------------------------------------------------------------- 3a. batched solving
- * Many independent LPs (no Q) solved by ONE persistent kernel: each thread
- * block owns one instance at a time (largest first) and runs the whole
- * restarted PDHG for it -- iterations, KKT checks, restarts, primal weight,
- * infeasibility test, FP32 phase then FP64 finish -- with block-level
- * synchronisation only.  opt->precision: GB_PREC_DOUBLE (FP64 throughout) or
- * GB_PREC_MIXED (FP32 matrix + iterates, FP64 finish); every result is
- * certified in FP64. */
+ * Many independent LPs (no Q) resident as ONE block-diagonal problem: every
+ * kernel launch covers all instances (a row block never straddles two), and
+ * each instance keeps its own scaling, step sizes, KKT checks, restarts,
+ * primal weight, infeasibility test, precision phases and FP64
+ * certification -- per-instance state lives on the device and a finished
+ * instance's row blocks return at once.  Each precision phase is one CUDA
+ * graph whose body repeats in a device-side loop.  opt->precision as for
+ * gb_solve; every result is certified in FP64. */
 typedef struct gb_batch gb_batch;
 int gb_batch_create(int count, const gb_lp* lps, const gb_options* opt, gb_batch** out);
 /* Solve every instance; results[count] receives per-instance results. */
@@ -254,6 +255,17 @@ int gb_batch_get_solution(gb_batch* b, int i, double* x_out, double* y_out);
  * the row-split group sizes picked per instance (written to groups[count*2]
  * when groups != NULL: group size for A rows, for A^T rows). */
 int gb_batch_schedule(gb_batch* b, int* threads, int* blocks_per_sm, int* groups);
+/* Row-split schedule autotuner: per class of instance sizes (four classes of
+ * equal total nonzeros), picks (block_nnz, max_rows) of the CSR row blocks by
+ * timing `iters` fused FP32 iterations per candidate with CUDA events.
+ * Writes the chosen values per instance (arrays of count, may be NULL) and
+ * the per-iteration kernel time of the default and the tuned schedule (ms). */
+int gb_batch_autotune(gb_batch* b, int iters, int* block_nnz, int* max_rows, double* ms_default, double* ms_tuned);
+/* Average device time of the two fused iteration kernels over `iters`
+ * iterations at a precision level (0 = FP32, 1 = FP32 matrix / FP64 vectors,
+ * 2 = FP64), all instances active, and the algorithmic bytes of one iteration. */
+int gb_batch_time_kernels(gb_batch* b, int level, int iters, double* ms_primal, double* ms_dual, int64_t* launches,
+                          double* bytes_per_iter);
 void gb_batch_destroy(gb_batch* b);
 
 /* ---------------------------------------------------------------- 3b. differentiable solving

@@ -65,3 +65,25 @@ def test_batch_schedule_report(batch):
         s = bs.schedule()
     assert s["threads"] == 256 and s["blocks_per_sm"] >= 1
     assert len(s["groups_A"]) == 4 and all(g in (1, 2, 4, 8, 16, 32) for g in s["groups_A"])
+
+
+def test_autotuned_schedules_keep_every_result(batch):
+    """The autotuner only re-cuts row blocks: verdicts stay those of the oracle,
+    every result stays certified, and the tuned iteration is not slower."""
+    import ganit_v2_b200 as gb
+
+    opt = gb.Options(precision=gb.Precision.Mixed)
+    with gb.BatchSolver(batch) as bs:
+        before = bs.solve(opt)
+        t = bs.autotune(iters=10)
+        assert set(t["block_nnz"].tolist()) <= {2048, 1024, 512}
+        assert set(t["max_rows"].tolist()) <= {256, 128, 64, 32}
+        assert t["ms_per_iter_tuned"] <= 1.05 * t["ms_per_iter_default"]
+        after = bs.solve(opt)
+        for i, (a, b) in enumerate(zip(before, after)):
+            assert a.status == b.status, i
+            if b.status_name == "OPTIMAL":
+                assert max(b.rel_primal, b.rel_dual, b.rel_gap) <= 1e-4 * 1.0000001
+                assert abs(a.pobj - b.pobj) <= 1e-3 * (1 + abs(a.pobj))
+        k = bs.time_kernels(0, 20)
+        assert k["ms_primal"] > 0 and k["ms_dual"] > 0 and k["bytes_per_iter"] > 0
