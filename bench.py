@@ -595,7 +595,8 @@ def main():
                          "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
                          "algorithmic_bytes_per_launch": dom[1]},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "status": re2e.status_name, "note": "gb_solve: upload + device scaling + solve + download"},
+                    "status": re2e.status_name, "setup_s_last": re2e.setup_seconds, "solve_s_last": re2e.solve_seconds,
+                    "note": "gb_solve: upload + device scaling + solve + download"},
             "gpu_launches": launches,
             "clocks": clk,
             "cpu_baseline": cpu,

@@ -147,7 +147,7 @@ class GbKkt(C.Structure):
 
 # Every symbol of include/ganit_b200.h (checked by the tests).
 EXPORTS = [
-    "gb_last_error", "gb_version", "gb_default_options", "gb_set_device", "gb_solve", "gb_problem_create",
+    "gb_last_error", "gb_release_cached_memory", "gb_cached_memory_bytes", "gb_version", "gb_default_options", "gb_set_device", "gb_solve", "gb_problem_create",
     "gb_problem_solve", "gb_problem_get_solution", "gb_problem_destroy", "gb_problem_stream",
     "gb_problem_time_kernels", "gb_problem_stats", "gb_backend_create", "gb_backend_destroy", "gb_vec_zeros",
     "gb_vec_from_host", "gb_vec_to_host", "gb_vec_size", "gb_vec_destroy", "gb_copy", "gb_fill", "gb_spmv_A",
@@ -172,7 +172,8 @@ def load_library(path: str = LIB_PATH):
     lib = C.CDLL(path)
     vp, i32, i64, dbl = C.c_void_p, C.c_int, C.c_int64, C.c_double
     sig = {
-        "gb_last_error": (C.c_char_p, []), "gb_version": (i32, []), "gb_default_options": (None, [vp]),
+        "gb_last_error": (C.c_char_p, []), "gb_release_cached_memory": (None, []),
+        "gb_cached_memory_bytes": (i64, []), "gb_version": (i32, []), "gb_default_options": (None, [vp]),
         "gb_set_device": (i32, [i32]), "gb_solve": (i32, [vp, vp, vp, vp, vp]),
         "gb_problem_create": (i32, [vp, vp, vp]), "gb_problem_solve": (i32, [vp, vp, vp]),
         "gb_problem_get_solution": (i32, [vp, vp, vp]), "gb_problem_destroy": (None, [vp]),
@@ -253,6 +254,15 @@ def _result(r: _GbResult, x, y) -> Result:
     return Result(Status(r.status), x, y, r.pobj, r.dobj, r.rel_primal, r.rel_dual, r.rel_gap, r.iterations,
                   r.fp32_iterations, r.l2_iterations, r.restarts, r.setup_seconds, r.solve_seconds, "b200",
                   r.norm_a, r.primal_weight, r.checks, r.phases)
+
+
+def release_cached_memory() -> None:
+    """Return the device blocks the library keeps for reuse to the driver."""
+    load_library().gb_release_cached_memory()
+
+
+def cached_memory_bytes() -> int:
+    return int(load_library().gb_cached_memory_bytes())
 
 
 def set_device(device: int) -> None:

@@ -34,6 +34,13 @@ struct Error : std::runtime_error {
         if (!(cond)) throw ::gb::Error(-1, std::string(msg));        \
     } while (0)
 
+// Device memory of the library (gb_pool.cu): cudaMalloc / cudaFree behind a
+// per-process cache of freed blocks (same device, same rounded size), so
+// that creating and destroying problems of the same shape -- the one-shot
+// gb_solve path -- does not pay the driver's allocation cost each time.
+void* dev_alloc(size_t bytes);
+void dev_free(void* p);
+
 // Owning device buffer (move-only).
 template <class T>
 class DevBuf {
@@ -52,10 +59,10 @@ class DevBuf {
     void reset(size_t n) {
         release();
         n_ = n;
-        if (n_) GB_CUDA(cudaMalloc(&p_, n_ * sizeof(T)));
+        if (n_) p_ = static_cast<T*>(dev_alloc(n_ * sizeof(T)));
     }
     void release() {
-        if (p_) cudaFree(p_);
+        if (p_) dev_free(p_);
         p_ = nullptr;
         n_ = 0;
     }

@@ -31,6 +31,7 @@ struct DevMat {
         v.counters = sched.counters.get();
         v.rows = rows;
         v.nb = sched.nb;
+        v.vec = 1;  // upload_mat / device_transpose / cvt32 allocate padded_nnz, cudaMalloc aligns
         return v;
     }
     template <class M>

@@ -172,10 +172,25 @@ struct CsrView {
     unsigned* counters;
     int rows;
     int nb;
+    // 1: idx / val are 16-byte aligned and readable 3 elements past the last
+    // nonzero (allocated with padded_nnz), so STREAM blocks use 16-byte loads.
+    // Views of caller-owned arrays leave it 0 (scalar loads).
+    int vec = 0;
 };
 
-// Padded element count of idx / val arrays used in persistent mode.
+// Element count of idx / val arrays allocated for 16-byte loads (CsrView::vec).
 inline long long padded_nnz(long long nnz) { return ((nnz + 3) & ~3LL) + 4; }
+
+// Four consecutive matrix values from a 16-byte-aligned address.
+__device__ __forceinline__ void load4(const float* p, float (&o)[4]) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+__device__ __forceinline__ void load4(const double* p, double (&o)[4]) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
 
 // Gather of a single right-hand side.
 template <class V>
@@ -306,14 +321,39 @@ __device__ __forceinline__ void spmv_run(const CsrView<M>& A, int cta, const Gat
         if ((tid & ((1 << b.lg) - 1)) == 0) pre = epi.prefetch(r);
     }
     const int cnt = b.p1 - b.p0;
-#pragma unroll 4
-    for (int k = tid; k < cnt; k += kThreads) {
-        const int p = b.p0 + k;
-        const V a = static_cast<V>(__ldg(A.val + p));
-        V xv[NV];
-        g(__ldg(A.idx + p), xv);
+    if (A.vec) {
+        // 16-byte loads over the 4-aligned window around [p0, p1); lanes of a
+        // group outside the block neither gather nor store.  (Loading two
+        // groups ahead of their gathers needs more registers than the 6-8
+        // resident CTAs per SM leave once the epilogue operands are in flight.)
+        const int q0 = b.p0 >> 2, q1 = (b.p1 + 3) >> 2;
+#pragma unroll 1
+        for (int q = q0 + tid; q < q1; q += kThreads) {
+            const int4 j4 = __ldg(reinterpret_cast<const int4*>(A.idx) + q);
+            M a4[4];
+            load4(A.val + 4 * q, a4);
+            const int js[4] = {j4.x, j4.y, j4.z, j4.w};
 #pragma unroll
-        for (int v = 0; v < NV; ++v) prod[v * kProdStride + padded(k)] = a * xv[v];
+            for (int e = 0; e < 4; ++e) {
+                const int k = 4 * q + e - b.p0;
+                if (k >= 0 && k < cnt) {
+                    V xv[NV];
+                    g(js[e], xv);
+#pragma unroll
+                    for (int v = 0; v < NV; ++v) prod[v * kProdStride + padded(k)] = static_cast<V>(a4[e]) * xv[v];
+                }
+            }
+        }
+    } else {
+#pragma unroll 4
+        for (int k = tid; k < cnt; k += kThreads) {
+            const int p = b.p0 + k;
+            const V a = static_cast<V>(__ldg(A.val + p));
+            V xv[NV];
+            g(__ldg(A.idx + p), xv);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) prod[v * kProdStride + padded(k)] = a * xv[v];
+        }
     }
     __syncthreads();
     reduce_rows<NV, V>(b, prod, s, e, act, pre, epi);

@@ -97,3 +97,25 @@ def test_invalid_problem_is_an_error_not_a_crash(gb):
     nan = gb.LP(lp.A, np.full(lp.n, np.nan), lp.l, lp.u, lp.lo, lp.hi)
     r = gb.solve_pdhg_gpu(nan, gb.Options(max_iter=640))
     assert r.status in (gb.Status.NumericalError, gb.Status.IterationLimit)
+
+
+def test_device_memory_cache_reuses_blocks_and_keeps_results():
+    """Freed device blocks are kept and reused by the next problem of the same
+    shape; the solve is unchanged and the cache can be emptied."""
+    import ganit_v2_b200 as gb
+    from ganit_v2_b200 import api, workloads as W
+
+    lp = W.random_feasible_lp(300, 700, 5, seed=21)
+    opt = gb.Options(precision=gb.Precision.Mixed)
+    api.release_cached_memory()
+    assert api.cached_memory_bytes() == 0
+    r1 = gb.solve_pdhg_gpu(lp, opt)
+    kept = api.cached_memory_bytes()
+    assert kept > 0
+    r2 = gb.solve_pdhg_gpu(lp, opt)
+    assert api.cached_memory_bytes() == kept  # same shape: every block came from the cache and went back
+    assert r1.status == r2.status and r1.iterations == r2.iterations
+    np.testing.assert_array_equal(r1.x, r2.x)
+    np.testing.assert_array_equal(r1.y, r2.y)
+    api.release_cached_memory()
+    assert api.cached_memory_bytes() == 0
