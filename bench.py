@@ -267,6 +267,16 @@ def batch_measure(dist, rank: int, world: int, steps: int = 3, seq_sample: int =
         res = bs.solve(mixed, fetch=False)
         secs.append(time.perf_counter() - t0)
     t_batch = reduce_max(dist, min(secs))
+    bf16 = gb.Options(precision=gb.Precision.MixedBf16)
+    res_bf = bs.solve(bf16, fetch=False)
+    torch.cuda.synchronize()
+    barrier(dist)
+    t0 = time.perf_counter()
+    res_bf = bs.solve(bf16, fetch=False)
+    t_bf = reduce_max(dist, time.perf_counter() - t0)
+    cert_bf = reduce_sum(dist, sum(r.status == gb.Status.Optimal and
+                                   max(r.rel_primal, r.rel_dual, r.rel_gap) <= 1e-4 * 1.0000001 for r in res_bf))
+    ktb = bs.time_kernels(3, 50)
     kt = bs.time_kernels(0, 50)
     kt64 = bs.time_kernels(2, 20)
     sched = bs.schedule()
@@ -309,6 +319,9 @@ def batch_measure(dist, rank: int, world: int, steps: int = 3, seq_sample: int =
                                   "frac_f64": gbs64 / peak, "peak": peak, "peak_source": f"{peak_kind} hbm_gbs",
                                   "note": "k_primal + k_dual over all instances (rank 0's shard), CUDA events, "
                                           "every instance active; bytes = 2 nnz (s_M+4) + 4 (m+n+2) + s_V (9n+7m)"},
+            "bf16_trial": {"lps_per_s": len(lps) / t_bf, "certified_1e-4": int(cert_bf),
+                           "ms_per_iter_bf16": ktb["ms_primal"] + ktb["ms_dual"],
+                           "gbs_bf16": ktb["bytes_per_iter"] / ((ktb["ms_primal"] + ktb["ms_dual"]) / 1e3) / 1e9},
             "autotune": {"seconds": tune_s, "ms_per_iter_default": tune["ms_per_iter_default"],
                          "ms_per_iter_tuned": tune["ms_per_iter_tuned"],
                          "choices": {f"{b}x{r}": int(np.sum((bn == b) & (mr == r)))
@@ -519,6 +532,11 @@ def main():
     barrier(dist)
     ms_fp64, r_fp64, _ = timed(fp64, max(1, args.steps // 2))
     torch.cuda.synchronize()
+    barrier(dist)
+    bf16 = gb.Options(precision=gb.Precision.MixedBf16)
+    prob.solve(bf16, fetch=False)
+    ms_bf16, r_bf16, _ = timed(bf16, max(1, args.steps // 2))
+    torch.cuda.synchronize()
     clk = clocks.stop()
     ms_mixed_max = reduce_max(dist, ms_mixed)
     ms_fp64_max = reduce_max(dist, ms_fp64)
@@ -528,10 +546,13 @@ def main():
     # kernel roofline: fused SpMV + step kernels at the FP32 level that dominates the mixed solve
     ms_p, ms_d, _ = prob.time_kernels(0, args.kernel_iters)
     ms_p64, ms_d64, _ = prob.time_kernels(2, args.kernel_iters)
+    ms_pbf, ms_dbf, _ = prob.time_kernels(3, args.kernel_iters)
     nnz, m, n = lp.A.nnz, lp.m, lp.n
     bytes_dual32 = nnz * 8 + 4 * (m + 1) + 4 * n + 4 * 6 * m
     bytes_primal32 = nnz * 8 + 4 * (n + 1) + 4 * m + 4 * 8 * n
     bytes_dual64 = nnz * 12 + 4 * (m + 1) + 8 * n + 8 * 6 * m
+    bytes_dualbf = nnz * 6 + 4 * (m + 1) + 4 * n + 4 * 6 * m
+    bytes_primalbf = nnz * 6 + 4 * (n + 1) + 4 * m + 4 * 8 * n
     bytes_primal64 = nnz * 12 + 4 * (n + 1) + 8 * m + 8 * 8 * n
     peak, peak_kind = measured_peaks()
     dom = ("k_dual<float,float>", bytes_dual32, ms_d) if ms_d >= ms_p else ("k_primal<float,float>", bytes_primal32, ms_p)
@@ -590,7 +611,16 @@ def main():
                          "k_dual_f32": bytes_dual32 / (ms_d / 1e3) / 1e9,
                          "k_primal_f64": bytes_primal64 / (ms_p64 / 1e3) / 1e9,
                          "k_dual_f64": bytes_dual64 / (ms_d64 / 1e3) / 1e9,
-                         "ms": {"primal_f32": ms_p, "dual_f32": ms_d, "primal_f64": ms_p64, "dual_f64": ms_d64}},
+                         "k_primal_bf16": bytes_primalbf / (ms_pbf / 1e3) / 1e9,
+                         "k_dual_bf16": bytes_dualbf / (ms_dbf / 1e3) / 1e9,
+                         "ms": {"primal_f32": ms_p, "dual_f32": ms_d, "primal_f64": ms_p64, "dual_f64": ms_d64,
+                                "primal_bf16": ms_pbf, "dual_bf16": ms_dbf}},
+            "bf16_trial": {"value": max(1, args.steps // 2) / (ms_bf16 / 1e3), "unit": UNIT,
+                           "ms_per_step": ms_bf16 / max(1, args.steps // 2), "status": r_bf16.status_name,
+                           "iterations": r_bf16.iterations, "bf16_iterations": r_bf16.bf16_iterations,
+                           "fp32_iterations": r_bf16.fp32_iterations, "pobj": r_bf16.pobj,
+                           "note": "GB_PREC_MIXED_BF16: BF16 matrix values + FP32 iterates until the phase stalls, "
+                                   "then FP32, then FP64; FP64-certified"},
             "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
                          "algorithmic_bytes_per_launch": dom[1]},

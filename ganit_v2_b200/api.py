@@ -39,6 +39,7 @@ class Precision(enum.IntEnum):  # include/ganit/pdhg.hpp:10
     Double = 0
     Mixed = 1
     Dynamic = 2
+    MixedBf16 = 3  # extension: BF16-matrix phase first (LPs)
 
 
 class Status(enum.IntEnum):  # include/ganit/pdhg.hpp:27
@@ -88,6 +89,7 @@ class Result:  # include/ganit/pdhg.hpp:30-42
     primal_weight: float = float("nan")
     checks: int = 0
     phases: int = 0
+    bf16_iterations: int = 0
 
     @property
     def status_name(self) -> str:
@@ -115,7 +117,8 @@ class _GbResult(C.Structure):
                 ("rel_dual", C.c_double), ("rel_gap", C.c_double), ("iterations", C.c_int64),
                 ("fp32_iterations", C.c_int64), ("l2_iterations", C.c_int64), ("restarts", C.c_int32),
                 ("setup_seconds", C.c_double), ("solve_seconds", C.c_double), ("norm_a", C.c_double),
-                ("primal_weight", C.c_double), ("checks", C.c_int32), ("phases", C.c_int32)]
+                ("primal_weight", C.c_double), ("checks", C.c_int32), ("phases", C.c_int32),
+                ("bf16_iterations", C.c_int64)]
 
 
 class _GbScaledLp(C.Structure):
@@ -253,7 +256,7 @@ def _opts(opt: Options | None) -> _GbOptions:
 def _result(r: _GbResult, x, y) -> Result:
     return Result(Status(r.status), x, y, r.pobj, r.dobj, r.rel_primal, r.rel_dual, r.rel_gap, r.iterations,
                   r.fp32_iterations, r.l2_iterations, r.restarts, r.setup_seconds, r.solve_seconds, "b200",
-                  r.norm_a, r.primal_weight, r.checks, r.phases)
+                  r.norm_a, r.primal_weight, r.checks, r.phases, r.bf16_iterations)
 
 
 def release_cached_memory() -> None:

@@ -3,6 +3,7 @@
 // vector update rounds exactly like the reference's scalar C++ code
 // (src/backend_cpu.cpp), i.e. no silent FMA contraction.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>

@@ -418,9 +418,30 @@ template <>
 VecSet<double>& Level<float, double>::vs(Problem& P) { return P.v64; }
 template <>
 VecSet<double>& Level<double, double>::vs(Problem& P) { return P.v64; }
+template <>
+VecSet<float>& Level<__nv_bfloat16, float>::vs(Problem& P) { return P.v32; }
 template <class M, class V>
 constexpr int level_index() {
-    return std::is_same<M, double>::value ? 2 : (std::is_same<V, double>::value ? 1 : 0);
+    return std::is_same<M, __nv_bfloat16>::value
+               ? 3
+               : (std::is_same<M, double>::value ? 2 : (std::is_same<V, double>::value ? 1 : 0));
+}
+
+// BF16 copies of the scaled matrix values (A and A^T), made once.  After
+// Ruiz / Pock-Chambolle scaling every value is O(1), far inside BF16's
+// (FP32's) exponent range; what BF16 gives up is precision (8-bit
+// significand), so its phase ends by the same stall rule as the FP32 one.
+void ensure_bf16(Problem& P) {
+    auto cvt = [&](DevMat& M) {
+        if (M.valbf.get()) return;
+        M.valbf.reset(padded_nnz(M.nnz));
+        if (M.nnz)
+            k_convert<__nv_bfloat16><<<elem_grid(M.nnz, P.sms), kThreads, 0, P.stream>>>(M.nnz, M.val64.get(),
+                                                                                        M.valbf.get());
+    };
+    cvt(P.A);
+    cvt(P.AT);
+    GB_CUDA(cudaGetLastError());
 }
 
 template <class M, class V>
@@ -710,7 +731,7 @@ int status_from(int e) {  // pdhg_impl.hpp:232-240
 // run_pdhg (pdhg_impl.hpp:243-328) of every instance with device-resident state.
 void solve_problem(Problem& P, const gb_options* opt, gb_result* res) {
     GB_REQUIRE(opt->check_every > 0, "check_every must be positive");
-    GB_REQUIRE(opt->precision >= 0 && opt->precision <= 2, "unknown precision");
+    GB_REQUIRE(opt->precision >= 0 && opt->precision <= 3, "unknown precision");
     GB_CUDA(cudaSetDevice(P.device));
     cudaStream_t s = P.stream;
     const auto t0 = std::chrono::steady_clock::now();
@@ -748,9 +769,20 @@ void solve_problem(Problem& P, const gb_options* opt, gb_result* res) {
     };
     if (opt->precision != GB_PREC_DOUBLE) {
         set_flags([](int) { return true; });
-        run_phase<float, float>(P, opt, opt->tol, 1, opt->stall_checks, true, false);
-        collect();
-        for (int k = 0; k < K; ++k) P.results[k].fp32_iters = P.st_host[k].it;
+        bool first = true;
+        if (opt->precision == GB_PREC_MIXED_BF16 && !P.has_q) {
+            ensure_bf16(P);
+            run_phase<__nv_bfloat16, float>(P, opt, opt->tol, 1, opt->stall_checks, true, false);
+            collect();
+            for (int k = 0; k < K; ++k) P.results[k].bf16_iters = P.st_host[k].it;
+            finished();
+            first = false;
+        }
+        if (set_flags([&](int k) { return !done[k]; })) {
+            run_phase<float, float>(P, opt, opt->tol, 1, opt->stall_checks, first, !first);
+            collect();
+        }
+        for (int k = 0; k < K; ++k) P.results[k].fp32_iters = P.st_host[k].it - P.results[k].bf16_iters;
         finished();
         if (opt->precision == GB_PREC_DYNAMIC && set_flags([&](int k) { return !done[k]; })) {
             run_phase<float, double>(P, opt, opt->tol, 1, opt->stall_checks_l2, false, true);
@@ -796,6 +828,7 @@ void solve_problem(Problem& P, const gb_options* opt, gb_result* res) {
         r.iterations = st.it;
         r.fp32_iterations = P.results[k].fp32_iters;
         r.l2_iterations = P.results[k].l2_iters;
+        r.bf16_iterations = P.results[k].bf16_iters;
         r.restarts = st.restarts;
         r.setup_seconds = P.setup_seconds;
         r.solve_seconds = solve_s;
@@ -1022,12 +1055,17 @@ void* gb_problem_stream(gb_problem* p) { return p ? static_cast<void*>(p->p->str
 int gb_problem_time_kernels(gb_problem* p, int level, int iters, double* ms_primal, double* ms_dual,
                             int64_t* launches) {
     return guarded([&] {
-        GB_REQUIRE(p && iters > 0 && level >= 0 && level <= 2, "bad arguments");
+        GB_REQUIRE(p && iters > 0 && level >= 0 && level <= 3, "bad arguments");
         Problem& P = *p->p;
         GB_REQUIRE(P.solved, "solve once before timing (step sizes come from the solve)");
+        GB_REQUIRE(level != 3 || !P.has_q, "the BF16 level takes LPs only");
         if (level == 0) time_level<float, float>(P, iters, ms_primal, ms_dual, launches);
         else if (level == 1) time_level<float, double>(P, iters, ms_primal, ms_dual, launches);
-        else time_level<double, double>(P, iters, ms_primal, ms_dual, launches);
+        else if (level == 2) time_level<double, double>(P, iters, ms_primal, ms_dual, launches);
+        else {
+            ensure_bf16(P);
+            time_level<__nv_bfloat16, float>(P, iters, ms_primal, ms_dual, launches);
+        }
     });
 }
 
@@ -1133,15 +1171,20 @@ int gb_batch_autotune(gb_batch* b, int iters, int* block_nnz, int* max_rows, dou
 int gb_batch_time_kernels(gb_batch* b, int level, int iters, double* ms_primal, double* ms_dual, int64_t* launches,
                           double* bytes_per_iter) {
     return guarded([&] {
-        GB_REQUIRE(b && iters > 0 && level >= 0 && level <= 2, "bad arguments");
+        GB_REQUIRE(b && iters > 0 && level >= 0 && level <= 3, "bad arguments");
         Problem& P = *b->p;
         if (level == 0) time_level<float, float>(P, iters, ms_primal, ms_dual, launches);
         else if (level == 1) time_level<float, double>(P, iters, ms_primal, ms_dual, launches);
-        else time_level<double, double>(P, iters, ms_primal, ms_dual, launches);
+        else if (level == 2) time_level<double, double>(P, iters, ms_primal, ms_dual, launches);
+        else {
+            ensure_bf16(P);
+            time_level<__nv_bfloat16, float>(P, iters, ms_primal, ms_dual, launches);
+        }
         if (bytes_per_iter) {
             double bpi[3];
             problem_stats(P, nullptr, bpi);
-            *bytes_per_iter = bpi[level];
+            // BF16 level: 2 bytes per matrix value instead of FP32's 4
+            *bytes_per_iter = level < 3 ? bpi[level] : bpi[0] - 2.0 * 2.0 * static_cast<double>(P.A.nnz);
         }
     });
 }

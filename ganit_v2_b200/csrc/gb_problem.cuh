@@ -18,6 +18,7 @@ struct DevMat {
     DevBuf<int> ptr, idx;
     DevBuf<double> val64;
     DevBuf<float> val32;
+    DevBuf<__nv_bfloat16> valbf;  // made on the first solve that asks for the BF16 phase
     DevSchedule sched;
     std::vector<int> host_ptr;
     template <class M>
@@ -41,6 +42,8 @@ template <>
 inline const double* DevMat::val<double>() const { return val64.get(); }
 template <>
 inline const float* DevMat::val<float>() const { return val32.get(); }
+template <>
+inline const __nv_bfloat16* DevMat::val<__nv_bfloat16>() const { return valbf.get(); }
 
 // Problem data and iterate buffers in vector precision V.
 template <class V>
@@ -76,7 +79,7 @@ struct LevelGraph {
 // Per-instance outcome of a solve.
 struct InstanceResult {
     int status = GB_NUMERICAL_ERROR;
-    long long fp32_iters = 0, l2_iters = 0;
+    long long bf16_iters = 0, fp32_iters = 0, l2_iters = 0;
     int phases = 0;
 };
 
@@ -110,7 +113,7 @@ struct Problem {
     int* phase_flags_host = nullptr;      // pinned
     DevBuf<unsigned> arrive;              // k_eval arrival counter
     DevBuf<double> partials;
-    std::unique_ptr<LevelGraph> graphs[3];
+    std::unique_ptr<LevelGraph> graphs[4];  // levels <f32,f32>, <f32,f64>, <f64,f64>, <bf16,f32>
     double setup_seconds = 0.0;
     long long launches = 0;               // kernel launches of the last solve
     std::vector<InstanceResult> results;

@@ -186,6 +186,12 @@ __device__ __forceinline__ void load4(const float* p, float (&o)[4]) {
     const float4 v = __ldg(reinterpret_cast<const float4*>(p));
     o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
 }
+__device__ __forceinline__ void load4(const __nv_bfloat16* p, __nv_bfloat16 (&o)[4]) {
+    const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));  // 8 bytes; 4q elements are 8-byte aligned
+    const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&v.x);
+    const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162*>(&v.y);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
 __device__ __forceinline__ void load4(const double* p, double (&o)[4]) {
     const double2 a = __ldg(reinterpret_cast<const double2*>(p));
     const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);

@@ -49,7 +49,11 @@ enum {
 enum { GB_OPTIMAL = 0, GB_PRIMAL_INFEASIBLE = 1, GB_ITERATION_LIMIT = 2, GB_TIME_LIMIT = 3, GB_NUMERICAL_ERROR = 4 };
 
 /* ---- precision schedule, include/ganit/pdhg.hpp:10 (same order) */
-enum { GB_PREC_DOUBLE = 0, GB_PREC_MIXED = 1, GB_PREC_DYNAMIC = 2 };
+enum { GB_PREC_DOUBLE = 0, GB_PREC_MIXED = 1, GB_PREC_DYNAMIC = 2,
+       /* extension (no reference counterpart): a first phase with BF16 matrix
+        * values and FP32 iterates, then FP32, then FP64, each exit certified
+        * in FP64; LPs only (a QP starts at the FP32 phase) */
+       GB_PREC_MIXED_BF16 = 3 };
 
 /* ---- value types for gb_backend_create */
 enum { GB_F32 = 0, GB_F64 = 1 };
@@ -108,6 +112,7 @@ typedef struct {
     double primal_weight; /* final primal weight w */
     int32_t checks;       /* KKT checks performed */
     int32_t phases;       /* precision phases run */
+    int64_t bf16_iterations; /* iterations of the BF16-matrix phase (GB_PREC_MIXED_BF16) */
 } gb_result;
 
 /* ---------------------------------------------------------------- common */
@@ -144,7 +149,8 @@ int gb_problem_get_solution(gb_problem* p, double* x_out, double* y_out);
 void gb_problem_destroy(gb_problem* p);
 /* Stream the problem's work is issued on (a cudaStream_t). */
 void* gb_problem_stream(gb_problem* p);
-/* Kernel-level timing of one precision level (0 = L1, 1 = L2, 2 = L3):
+/* Kernel-level timing of one precision level (0 = L1, 1 = L2, 2 = L3,
+ * 3 = the BF16-matrix level of GB_PREC_MIXED_BF16, LPs only):
  * runs `iters` plain PDHG iterations from the current iterate with CUDA
  * events around every launch and reports the mean duration (ms) of the fused
  * primal kernel (A^T y + primal step) and of the fused dual kernel (A xbar +
@@ -271,6 +277,7 @@ int gb_batch_schedule(gb_batch* b, int* threads, int* blocks_per_sm, int* groups
 int gb_batch_autotune(gb_batch* b, int iters, int* block_nnz, int* max_rows, double* ms_default, double* ms_tuned);
 /* Average device time of the two fused iteration kernels over `iters`
  * iterations at a precision level (0 = FP32, 1 = FP32 matrix / FP64 vectors,
+ * 3 = BF16 matrix / FP32 vectors,
  * 2 = FP64), all instances active, and the algorithmic bytes of one iteration. */
 int gb_batch_time_kernels(gb_batch* b, int level, int iters, double* ms_primal, double* ms_dual, int64_t* launches,
                           double* bytes_per_iter);

@@ -87,3 +87,18 @@ def test_autotuned_schedules_keep_every_result(batch):
                 assert abs(a.pobj - b.pobj) <= 1e-3 * (1 + abs(a.pobj))
         k = bs.time_kernels(0, 20)
         assert k["ms_primal"] > 0 and k["ms_dual"] > 0 and k["bytes_per_iter"] > 0
+
+
+def test_batch_with_bf16_phase_certifies_every_instance(batch, oracle_built):
+    import ganit_v2_b200 as gb
+
+    with gb.BatchSolver(batch) as bs:
+        res = bs.solve(gb.Options(precision=gb.Precision.MixedBf16))
+        for i, (lp, r) in enumerate(zip(batch, res)):
+            o = oracle_built.solve(lp, precision="mixed")
+            assert r.status_name == o.status, (i, lp.name)
+            if o.status == "OPTIMAL":
+                assert max(r.rel_primal, r.rel_dual, r.rel_gap) <= 1e-4 * 1.0000001
+                assert abs(r.pobj - o.pobj) <= 1e-3 * (1 + abs(o.pobj))
+        k = bs.time_kernels(3, 10)
+        assert k["ms_primal"] > 0 and k["bytes_per_iter"] > 0

@@ -119,3 +119,20 @@ def test_device_memory_cache_reuses_blocks_and_keeps_results():
     np.testing.assert_array_equal(r1.y, r2.y)
     api.release_cached_memory()
     assert api.cached_memory_bytes() == 0
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN["synthetic"]))
+def test_bf16_matrix_phase_reaches_the_reference_answer(gb, name):
+    """GB_PREC_MIXED_BF16 (an extension: BF16 matrix values first, then FP32,
+    then FP64) meets the same bar against the reference's mixed-precision
+    results: same verdict, FP64-certified KKT within tol, objective within
+    10 * tol.  QPs skip the BF16 phase."""
+    lp, _ = load_lp(os.path.join(GOLD, name + ".npz"))
+    entry = GOLDEN["synthetic"][name]
+    tol = entry["options"].get("tol", 1e-4)
+    r = gb.solve_pdhg_gpu(lp, gb.Options(tol=tol, precision=gb.Precision.MixedBf16))
+    check_against(r, entry["results"]["mixed"], tol, "mixed")
+    if lp.Q is None:
+        assert r.bf16_iterations > 0
+    else:
+        assert r.bf16_iterations == 0
