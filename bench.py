@@ -324,6 +324,12 @@ def batch_measure(dist, rank: int, world: int, steps: int = 3, seq_sample: int =
                            "gbs_bf16": ktb["bytes_per_iter"] / ((ktb["ms_primal"] + ktb["ms_dual"]) / 1e3) / 1e9},
             "autotune": {"seconds": tune_s, "ms_per_iter_default": tune["ms_per_iter_default"],
                          "ms_per_iter_tuned": tune["ms_per_iter_tuned"],
+                         "ms_per_iter_default_f64": tune["ms_per_iter_default_f64"],
+                         "ms_per_iter_tuned_f64": tune["ms_per_iter_tuned_f64"],
+                         "choices_f64": {f"{b}x{r}": int(np.sum((tune["block_nnz_f64"] == b) &
+                                                                (tune["max_rows_f64"] == r)))
+                                         for b, r in sorted(set(zip(tune["block_nnz_f64"].tolist(),
+                                                                    tune["max_rows_f64"].tolist())))},
                          "choices": {f"{b}x{r}": int(np.sum((bn == b) & (mr == r)))
                                      for b, r in sorted(set(zip(bn.tolist(), mr.tolist())))}},
             "schedule": {"threads": sched["threads"], "blocks_per_sm": sched["blocks_per_sm"],

@@ -152,7 +152,7 @@ class GbKkt(C.Structure):
 EXPORTS = [
     "gb_last_error", "gb_release_cached_memory", "gb_cached_memory_bytes", "gb_version", "gb_default_options", "gb_set_device", "gb_solve", "gb_problem_create",
     "gb_problem_solve", "gb_problem_get_solution", "gb_problem_destroy", "gb_problem_stream",
-    "gb_problem_time_kernels", "gb_problem_stats", "gb_backend_create", "gb_backend_destroy", "gb_vec_zeros",
+    "gb_problem_time_kernels", "gb_problem_stats", "gb_problem_autotune", "gb_backend_create", "gb_backend_destroy", "gb_vec_zeros",
     "gb_vec_from_host", "gb_vec_to_host", "gb_vec_size", "gb_vec_destroy", "gb_copy", "gb_fill", "gb_spmv_A",
     "gb_spmv_AT", "gb_spmv_Q", "gb_primal_step", "gb_dual_step", "gb_sub", "gb_scale_into", "gb_primal_res2",
     "gb_dual_res", "gb_row_dual_obj", "gb_dot", "gb_dot_c", "gb_diff2", "gb_batch_create", "gb_batch_solve",
@@ -181,7 +181,7 @@ def load_library(path: str = LIB_PATH):
         "gb_problem_create": (i32, [vp, vp, vp]), "gb_problem_solve": (i32, [vp, vp, vp]),
         "gb_problem_get_solution": (i32, [vp, vp, vp]), "gb_problem_destroy": (None, [vp]),
         "gb_problem_stream": (vp, [vp]), "gb_problem_time_kernels": (i32, [vp, i32, i32, vp, vp, vp]),
-        "gb_problem_stats": (i32, [vp, vp, vp]), "gb_backend_create": (i32, [vp, i32, i32, vp]),
+        "gb_problem_stats": (i32, [vp, vp, vp]), "gb_problem_autotune": (i32, [vp, i32, vp, vp, vp, vp]), "gb_backend_create": (i32, [vp, i32, i32, vp]),
         "gb_backend_destroy": (None, [vp]), "gb_vec_zeros": (i32, [vp, i32, vp]),
         "gb_vec_from_host": (i32, [vp, vp, i32, vp]), "gb_vec_to_host": (i32, [vp, vp, vp]),
         "gb_vec_size": (i32, [vp]), "gb_vec_destroy": (None, [vp]), "gb_copy": (i32, [vp, vp, vp]),
@@ -325,6 +325,15 @@ class Problem:
                                                  C.byref(nl)))
         return mp.value, md.value, nl.value
 
+    def autotune(self, iters: int = 50) -> dict:
+        """Pick the row-block cut by timing (gb_problem_autotune); solve once first."""
+        bn, mr = np.zeros(2, dtype=np.int32), np.zeros(2, dtype=np.int32)
+        t0, t1 = np.zeros(2), np.zeros(2)
+        _check(self._lib.gb_problem_autotune(self._h, int(iters), _p(bn), _p(mr), _p(t0), _p(t1)))
+        return {"block_nnz": int(bn[0]), "max_rows": int(mr[0]), "ms_per_iter_default": float(t0[0]),
+                "ms_per_iter_tuned": float(t1[0]), "block_nnz_f64": int(bn[1]), "max_rows_f64": int(mr[1]),
+                "ms_per_iter_default_f64": float(t0[1]), "ms_per_iter_tuned_f64": float(t1[1])}
+
     def stats(self):
         nl = C.c_int64()
         bpi = np.zeros(3)
@@ -402,11 +411,13 @@ class BatchSolver:
     def autotune(self, iters: int = 30) -> dict:
         """Pick row-split schedules per instance-size class by timing (gb_batch_autotune)."""
         k = len(self.lps)
-        bn = np.zeros(k, dtype=np.int32)
-        mr = np.zeros(k, dtype=np.int32)
-        t0, t1 = C.c_double(), C.c_double()
-        _check(self._lib.gb_batch_autotune(self._h, int(iters), _p(bn), _p(mr), C.byref(t0), C.byref(t1)))
-        return {"block_nnz": bn, "max_rows": mr, "ms_per_iter_default": t0.value, "ms_per_iter_tuned": t1.value}
+        bn = np.zeros(2 * k, dtype=np.int32)
+        mr = np.zeros(2 * k, dtype=np.int32)
+        t0, t1 = np.zeros(2), np.zeros(2)
+        _check(self._lib.gb_batch_autotune(self._h, int(iters), _p(bn), _p(mr), _p(t0), _p(t1)))
+        return {"block_nnz": bn[:k], "max_rows": mr[:k], "block_nnz_f64": bn[k:], "max_rows_f64": mr[k:],
+                "ms_per_iter_default": float(t0[0]), "ms_per_iter_tuned": float(t1[0]),
+                "ms_per_iter_default_f64": float(t0[1]), "ms_per_iter_tuned_f64": float(t1[1])}
 
     def time_kernels(self, level: int = 0, iters: int = 50) -> dict:
         """Device time of the fused iteration kernels with every instance active."""

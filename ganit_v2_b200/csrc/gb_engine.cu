@@ -7,6 +7,7 @@
 //                            each instance with its own scaling, step sizes,
 //                            restarts, primal weight, phases and certification
 #include <algorithm>
+#include <array>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -315,8 +316,10 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     GB_CUDA(cudaMemsetAsync(P->arrive.get(), 0, sizeof(unsigned), s));
 
     // schedules (host, from the row-length histogram, per instance) and transpose
-    P->tune_block_nnz.assign(count, kBlockNnz);
-    P->tune_max_rows.assign(count, kThreads);
+    for (int w = 0; w < 2; ++w) {
+        P->tune_block_nnz[w].assign(count, kBlockNnz);
+        P->tune_max_rows[w].assign(count, kThreads);
+    }
     P->A.sched.upload(build_schedule(P->A.host_ptr.data(), m, P->row_off.data(), count), 3, s);
     device_transpose(*P, s);
     P->AT.sched.upload(build_schedule(P->AT.host_ptr.data(), n, P->col_off.data(), count), 3, s);
@@ -499,12 +502,12 @@ EvalArgs<M, V> eval_args(Problem& P, VecSet<V>& vs, const V* x, const V* y, int 
     a.qxa = (with_q && mode == kEvalCheck) ? vs.qxa.get() : nullptr;
     a.mode = mode;
     a.count = P.count;
-    a.seg_a = P.A.sched.seg_block.get();
-    a.seg_t = P.AT.sched.seg_block.get();
+    a.seg_a = P.A.sched_for<M>().seg_block.get();
+    a.seg_t = P.AT.sched_for<M>().seg_block.get();
     a.st = P.st.get();
     a.arrive = P.arrive.get();
     a.partials = P.partials.get();
-    a.inst_terms = P.partials.get() + static_cast<size_t>(P.A.sched.nb + P.AT.sched.nb) * kTerms;
+    a.inst_terms = P.partials.get() + static_cast<size_t>(a.A.nb + a.AT.nb) * kTerms;
     a.cond = 0;
     a.use_cond = 0;
     return a;
@@ -521,11 +524,11 @@ void launch_iteration(Problem& P, VecSet<V>& vs, int k, cudaStream_t s, long lon
     constexpr size_t sm = spmv_smem_bytes<1, V>();
     PrimalArgs<M, V> pa{P.AT.view<M>(), yin, xin, vs.c.get(), vs.l.get(), vs.u.get(),
                         P.has_q ? vs.qx.get() : nullptr, xout, vs.xbar.get(), vs.sumx.get(), P.st.get()};
-    k_primal<M, V><<<P.AT.sched.nb, kThreads, sm, s>>>(pa);
+    k_primal<M, V><<<pa.AT.nb, kThreads, sm, s>>>(pa);
     if (mid) GB_CUDA(cudaEventRecord(mid, s));
     DualArgs<M, V> da{P.A.view<M>(), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(),
                       P.st.get()};
-    k_dual<M, V><<<P.A.sched.nb, kThreads, sm, s>>>(da);
+    k_dual<M, V><<<da.A.nb, kThreads, sm, s>>>(da);
     nl += 2;
 }
 
@@ -543,7 +546,7 @@ long long capture_body(Problem& P, int ce, cudaGraphConditionalHandle cond, cuda
     EvalArgs<M, V> ea = eval_args<M, V>(P, vs, xc, yc, kEvalCheck, P.has_q);
     ea.cond = cond;
     ea.use_cond = use_cond;
-    const int grid = P.A.sched.nb + P.AT.sched.nb;
+    const int grid = ea.A.nb + ea.AT.nb;
     k_eval<M, V, 2, 3><<<grid, kThreads, spmv_smem_bytes<3, V>(), s>>>(ea);
     RestartArgs<V> ra{xc, yc, vs.x0.get(), vs.y0.get(), vs.xr.get(), vs.yr.get(), vs.sumx.get(), vs.sumy.get(),
                       P.n, P.m, P.icol(), P.irow(), P.st.get()};
@@ -672,7 +675,7 @@ void run_phase(Problem& P, const gb_options* opt, double tol, int stall_exit, in
     P.launches += 2;
     if (P.has_q) launch_qx<M, V>(P, vs, vs.x0.get(), vs.qx.get(), s, P.launches);
     EvalArgs<M, V> ea = eval_args<M, V>(P, vs, vs.x0.get(), vs.y0.get(), kEvalInit, P.has_q);
-    k_eval<M, V, 1, 1><<<P.A.sched.nb + P.AT.sched.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(ea);
+    k_eval<M, V, 1, 1><<<ea.A.nb + ea.AT.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(ea);
     P.launches += 1;
     long long per_body = 0;
     long long bodies = 0;
@@ -711,7 +714,7 @@ void certify(Problem& P) {
     VecSet<double>& vs = P.v64;
     if (P.has_q) launch_qx<double, double>(P, vs, P.x64.get(), vs.qx.get(), s, P.launches);
     EvalArgs<double, double> ea = eval_args<double, double>(P, vs, P.x64.get(), P.y64.get(), kEvalCertify, P.has_q);
-    k_eval<double, double, 1, 1><<<P.A.sched.nb + P.AT.sched.nb, kThreads, spmv_smem_bytes<1, double>(), s>>>(ea);
+    k_eval<double, double, 1, 1><<<ea.A.nb + ea.AT.nb, kThreads, spmv_smem_bytes<1, double>(), s>>>(ea);
     P.launches += 1;
     sync_state(P);
 }
@@ -873,51 +876,74 @@ void time_level(Problem& P, int iters, double* msp, double* msd, int64_t* launch
     *launches = nl;
 }
 
-// Rebuild both schedules from the per-instance tunables; captured graphs
-// hold the old schedule and are dropped.
-void rebuild_schedules(Problem& P) {
+// Rebuild the row-block schedules of A and A^T for kernel class w (0: FP32 /
+// BF16 matrix, 1: FP64 matrix) from the per-instance tunables; captured
+// graphs hold the old schedules and are dropped.
+void rebuild_schedules(Problem& P, int w) {
     cudaStream_t s = P.stream;
     GB_CUDA(cudaStreamSynchronize(s));
     for (auto& g : P.graphs) g.reset();
-    P.A.sched.upload(build_schedule(P.A.host_ptr.data(), P.row_off.data(), P.count, P.tune_block_nnz.data(),
-                                    P.tune_max_rows.data()),
-                     3, s);
-    P.AT.sched.upload(build_schedule(P.AT.host_ptr.data(), P.col_off.data(), P.count, P.tune_block_nnz.data(),
-                                     P.tune_max_rows.data()),
-                      3, s);
-    const size_t need = static_cast<size_t>(P.A.sched.nb + P.AT.sched.nb + P.count) * kTerms;
+    DevSchedule& sa = w == 0 ? P.A.sched32 : P.A.sched;
+    DevSchedule& st = w == 0 ? P.AT.sched32 : P.AT.sched;
+    sa.upload(build_schedule(P.A.host_ptr.data(), P.row_off.data(), P.count, P.tune_block_nnz[w].data(),
+                             P.tune_max_rows[w].data()),
+              3, s);
+    st.upload(build_schedule(P.AT.host_ptr.data(), P.col_off.data(), P.count, P.tune_block_nnz[w].data(),
+                             P.tune_max_rows[w].data()),
+              3, s);
+    const int nb = std::max(P.A.sched.nb + P.AT.sched.nb, P.A.sched32.nb + P.AT.sched32.nb);
+    const size_t need = static_cast<size_t>(nb + P.count) * kTerms;
     if (P.partials.size() < need) P.partials.reset(need);
     GB_CUDA(cudaStreamSynchronize(s));
 }
 
-// Row-split schedule autotuner.  Instances are binned into (at most) four
+// Row-split schedule autotuner, run once per kernel class (w = 0: the FP32
+// schedule, timed with the FP32 iteration kernels; w = 1: the FP64 one,
+// timed with the FP64 kernels).  Instances are binned into (at most) four
 // classes of equal total nonzeros by instance size; for each class in turn
 // every candidate (block_nnz, max_rows) -- block_nnz bounds the nonzeros a
 // STREAM block stages (<= kBlockNnz, the shared-memory product buffer),
 // max_rows the rows it reduces and hence the lanes per row -- is tried with
-// the other classes at their incumbents, by timing `iters` fused FP32
-// iterations (CUDA events around k_primal + k_dual), and kept when it is
-// more than 1% faster.  The per-row group size inside a block still follows
-// the block's row count (the row-length histogram).
-void autotune(Problem& P, int iters, double* ms_default, double* ms_tuned) {
-    static const int cand[][2] = {{2048, 256}, {2048, 128}, {2048, 64}, {1024, 256}, {1024, 128},
-                                  {1024, 64},  {1024, 32},  {512, 64},  {512, 32}};
+// the other classes at their incumbents, by timing `iters` fused iterations
+// (CUDA events around k_primal + k_dual), and kept when it is more than 1%
+// faster.  The per-row group size inside a block still follows the block's
+// row count (the row-length histogram).  Besides a fixed grid of candidates,
+// block sizes that cut the nonzeros into whole waves of resident CTAs are
+// tried: a launch of 1.2 waves leaves most SMs idle during its second wave.
+void autotune_class(Problem& P, int w, int iters, double* ms_default, double* ms_tuned) {
+    std::vector<std::array<int, 2>> cand = {{2048, 256}, {2048, 128}, {2048, 64}, {1024, 256}, {1024, 128},
+                                            {1024, 64},  {1024, 32},  {512, 64},  {512, 32}};
+    int per_sm = 0;
+    if (w == 0)
+        GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dual<float, float>, kThreads,
+                                                              spmv_smem_bytes<1, float>()));
+    else
+        GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dual<double, double>, kThreads,
+                                                              spmv_smem_bytes<1, double>()));
+    const long long wave = static_cast<long long>(std::max(per_sm, 1)) * P.sms;
+    for (int k = 1; k <= 4; ++k) {
+        long long b = (P.A.nnz + k * wave - 1) / (k * wave);
+        b = (b + 31) / 32 * 32;
+        if (b >= 256 && b <= kBlockNnz) cand.push_back({static_cast<int>(b), kThreads});
+    }
     auto measure = [&]() {
         double best = INFINITY;
         for (int rep = 0; rep < 2; ++rep) {
             double mp = 0, md = 0;
             int64_t nl = 0;
-            time_level<float, float>(P, iters, &mp, &md, &nl);
+            if (w == 0) time_level<float, float>(P, iters, &mp, &md, &nl);
+            else time_level<double, double>(P, iters, &mp, &md, &nl);
             best = std::min(best, mp + md);
         }
         return best;
     };
-    P.tune_block_nnz.assign(P.count, kBlockNnz);
-    P.tune_max_rows.assign(P.count, kThreads);
-    rebuild_schedules(P);
+    auto& tb = P.tune_block_nnz[w];
+    auto& tr = P.tune_max_rows[w];
+    tb.assign(P.count, kBlockNnz);
+    tr.assign(P.count, kThreads);
+    rebuild_schedules(P, w);
     double best = measure();
     if (ms_default) *ms_default = best;
-    // classes by instance size
     std::vector<int> order(P.count);
     std::iota(order.begin(), order.end(), 0);
     auto nnz_of = [&](int k) { return static_cast<long long>(P.nnz_off[k + 1]) - P.nnz_off[k]; };
@@ -933,15 +959,15 @@ void autotune(Problem& P, int iters, double* ms_default, double* ms_tuned) {
     }
     for (const auto& members : cls) {
         if (members.empty()) continue;
-        const int inc_b = P.tune_block_nnz[members[0]], inc_r = P.tune_max_rows[members[0]];
+        const int inc_b = tb[members[0]], inc_r = tr[members[0]];
         int win_b = inc_b, win_r = inc_r;
         for (const auto& c : cand) {
             if (c[0] == inc_b && c[1] == inc_r) continue;
             for (int k : members) {
-                P.tune_block_nnz[k] = c[0];
-                P.tune_max_rows[k] = c[1];
+                tb[k] = c[0];
+                tr[k] = c[1];
             }
-            rebuild_schedules(P);
+            rebuild_schedules(P, w);
             const double t = measure();
             if (t < 0.99 * best) {
                 best = t;
@@ -950,12 +976,18 @@ void autotune(Problem& P, int iters, double* ms_default, double* ms_tuned) {
             }
         }
         for (int k : members) {
-            P.tune_block_nnz[k] = win_b;
-            P.tune_max_rows[k] = win_r;
+            tb[k] = win_b;
+            tr[k] = win_r;
         }
     }
-    rebuild_schedules(P);
+    rebuild_schedules(P, w);
     if (ms_tuned) *ms_tuned = measure();
+}
+
+// Both classes; outputs [FP32, FP64].
+void autotune(Problem& P, int iters, double* ms_default, double* ms_tuned) {
+    for (int w = 0; w < 2; ++w)
+        autotune_class(P, w, iters, ms_default ? ms_default + w : nullptr, ms_tuned ? ms_tuned + w : nullptr);
 }
 
 void problem_stats(const Problem& P, int64_t* launches, double* bpi) {
@@ -1138,9 +1170,11 @@ int gb_batch_schedule(gb_batch* b, int* threads, int* blocks_per_sm, int* groups
         }
         if (groups) {
             // group size (lanes per row) used by most of an instance's STREAM-block nonzeros
-            std::vector<RowBlock> ba(P.A.sched.nb), bt(P.AT.sched.nb);
-            P.A.sched.blocks.download(ba.data(), ba.size(), P.stream);
-            P.AT.sched.blocks.download(bt.data(), bt.size(), P.stream);
+            const DevSchedule& sa = P.A.sched_for<float>();
+            const DevSchedule& sb = P.AT.sched_for<float>();
+            std::vector<RowBlock> ba(sa.nb), bt(sb.nb);
+            sa.blocks.download(ba.data(), ba.size(), P.stream);
+            sb.blocks.download(bt.data(), bt.size(), P.stream);
             GB_CUDA(cudaStreamSynchronize(P.stream));
             auto mode_g = [](const std::vector<RowBlock>& bl, int b0, int b1) {
                 int cnt[6] = {0};
@@ -1149,8 +1183,8 @@ int gb_batch_schedule(gb_batch* b, int* threads, int* blocks_per_sm, int* groups
                 return 1 << static_cast<int>(std::max_element(cnt, cnt + 6) - cnt);
             };
             for (int k = 0; k < P.count; ++k) {
-                groups[2 * k] = mode_g(ba, P.A.sched.host_seg_block[k], P.A.sched.host_seg_block[k + 1]);
-                groups[2 * k + 1] = mode_g(bt, P.AT.sched.host_seg_block[k], P.AT.sched.host_seg_block[k + 1]);
+                groups[2 * k] = mode_g(ba, sa.host_seg_block[k], sa.host_seg_block[k + 1]);
+                groups[2 * k + 1] = mode_g(bt, sb.host_seg_block[k], sb.host_seg_block[k + 1]);
             }
         }
     });
@@ -1161,9 +1195,24 @@ int gb_batch_autotune(gb_batch* b, int iters, int* block_nnz, int* max_rows, dou
         GB_REQUIRE(b != nullptr && iters > 0, "bad arguments");
         Problem& P = *b->p;
         autotune(P, iters, ms_default, ms_tuned);
-        for (int k = 0; k < P.count; ++k) {
-            if (block_nnz) block_nnz[k] = P.tune_block_nnz[k];
-            if (max_rows) max_rows[k] = P.tune_max_rows[k];
+        for (int w = 0; w < 2; ++w)
+            for (int k = 0; k < P.count; ++k) {
+                if (block_nnz) block_nnz[w * P.count + k] = P.tune_block_nnz[w][k];
+                if (max_rows) max_rows[w * P.count + k] = P.tune_max_rows[w][k];
+            }
+    });
+}
+
+int gb_problem_autotune(gb_problem* p, int iters, int* block_nnz, int* max_rows, double* ms_default,
+                        double* ms_tuned) {
+    return guarded([&] {
+        GB_REQUIRE(p != nullptr && iters > 0, "bad arguments");
+        Problem& P = *p->p;
+        GB_REQUIRE(P.solved, "solve once before tuning (the iterate and step sizes come from the solve)");
+        autotune(P, iters, ms_default, ms_tuned);
+        for (int w = 0; w < 2; ++w) {
+            if (block_nnz) block_nnz[w] = P.tune_block_nnz[w][0];
+            if (max_rows) max_rows[w] = P.tune_max_rows[w][0];
         }
     });
 }

@@ -5,6 +5,7 @@
 #pragma once
 #include <chrono>
 #include <memory>
+#include <type_traits>
 
 #include "../../include/ganit_b200.h"
 #include "gb_pdhg.cuh"
@@ -19,19 +20,27 @@ struct DevMat {
     DevBuf<double> val64;
     DevBuf<float> val32;
     DevBuf<__nv_bfloat16> valbf;  // made on the first solve that asks for the BF16 phase
-    DevSchedule sched;
+    DevSchedule sched;    // row blocks of the FP64-matrix kernels (and of all kernels until tuned)
+    DevSchedule sched32;  // row blocks tuned for the FP32 / BF16-matrix kernels (empty: use sched)
     std::vector<int> host_ptr;
+    // The schedule the kernels of matrix type M run on: FP32 and BF16 kernels
+    // keep more CTAs resident per SM than FP64 ones, so the best cut differs.
+    template <class M>
+    const DevSchedule& sched_for() const {
+        return (!std::is_same<M, double>::value && sched32.nb) ? sched32 : sched;
+    }
     template <class M>
     CsrView<M> view() const {
+        const DevSchedule& sc = sched_for<M>();
         CsrView<M> v;
         v.ptr = ptr.get();
         v.idx = idx.get();
         v.val = val<M>();
-        v.blocks = sched.blocks.get();
-        v.slots = sched.slots.get();
-        v.counters = sched.counters.get();
+        v.blocks = sc.blocks.get();
+        v.slots = sc.slots.get();
+        v.counters = sc.counters.get();
         v.rows = rows;
-        v.nb = sched.nb;
+        v.nb = sc.nb;
         v.vec = 1;  // upload_mat / device_transpose / cvt32 allocate padded_nnz, cudaMalloc aligns
         return v;
     }
@@ -118,8 +127,9 @@ struct Problem {
     long long launches = 0;               // kernel launches of the last solve
     std::vector<InstanceResult> results;
     bool solved = false;
-    // row-split schedule tunables per instance (the batch autotuner sets them)
-    std::vector<int> tune_block_nnz, tune_max_rows;
+    // row-split schedule tunables per instance and schedule (index 0: FP32 /
+    // BF16 kernels, 1: FP64 kernels); set by the autotuner
+    std::vector<int> tune_block_nnz[2], tune_max_rows[2];
 
     const int* icol() const { return count > 1 ? inst_col.get() : nullptr; }
     const int* irow() const { return count > 1 ? inst_row.get() : nullptr; }

@@ -161,6 +161,15 @@ int gb_problem_time_kernels(gb_problem* p, int level, int iters, double* ms_prim
  * solve, and algorithmic bytes moved by the fused iteration kernels per
  * iteration at each level (index 0..2 = L1..L3). */
 int gb_problem_stats(gb_problem* p, int64_t* launches, double* bytes_per_iter_level);
+/* Row-split schedule autotuner for one resident problem (see
+ * gb_batch_autotune): after a first solve, times candidate (block_nnz,
+ * max_rows) cuts of the CSR row blocks -- including cuts into whole waves of
+ * resident CTAs -- separately for the FP32/BF16-matrix kernels and the FP64
+ * ones, and keeps the fastest of each.  Outputs are pairs [FP32, FP64]
+ * (block_nnz[2], max_rows[2], ms_default[2], ms_tuned[2]; any may be NULL).
+ * Results stay certified; only the summation grouping inside a row changes. */
+int gb_problem_autotune(gb_problem* p, int iters, int* block_nnz, int* max_rows, double* ms_default,
+                        double* ms_tuned);
 
 /* ---------------------------------------------------------------- 2. backend ops
  * Mirrors the Backend concept used at src/pdhg_impl.hpp:73-84, 92-118,
@@ -271,9 +280,11 @@ int gb_batch_get_solution(gb_batch* b, int i, double* x_out, double* y_out);
 int gb_batch_schedule(gb_batch* b, int* threads, int* blocks_per_sm, int* groups);
 /* Row-split schedule autotuner: per class of instance sizes (four classes of
  * equal total nonzeros), picks (block_nnz, max_rows) of the CSR row blocks by
- * timing `iters` fused FP32 iterations per candidate with CUDA events.
- * Writes the chosen values per instance (arrays of count, may be NULL) and
- * the per-iteration kernel time of the default and the tuned schedule (ms). */
+ * timing `iters` fused iterations per candidate with CUDA events -- once for
+ * the schedule of the FP32/BF16-matrix kernels (timed at FP32), once for that
+ * of the FP64 kernels (timed at FP64).  Writes the chosen values per instance
+ * (arrays of 2 * count: FP32 schedule then FP64; may be NULL) and the
+ * per-iteration kernel time of the default and tuned schedules (ms, [2]). */
 int gb_batch_autotune(gb_batch* b, int iters, int* block_nnz, int* max_rows, double* ms_default, double* ms_tuned);
 /* Average device time of the two fused iteration kernels over `iters`
  * iterations at a precision level (0 = FP32, 1 = FP32 matrix / FP64 vectors,

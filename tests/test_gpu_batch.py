@@ -76,9 +76,10 @@ def test_autotuned_schedules_keep_every_result(batch):
     with gb.BatchSolver(batch) as bs:
         before = bs.solve(opt)
         t = bs.autotune(iters=10)
-        assert set(t["block_nnz"].tolist()) <= {2048, 1024, 512}
+        assert all(256 <= b <= 2048 for b in t["block_nnz"].tolist() + t["block_nnz_f64"].tolist())
         assert set(t["max_rows"].tolist()) <= {256, 128, 64, 32}
         assert t["ms_per_iter_tuned"] <= 1.05 * t["ms_per_iter_default"]
+        assert t["ms_per_iter_tuned_f64"] <= 1.05 * t["ms_per_iter_default_f64"]
         after = bs.solve(opt)
         for i, (a, b) in enumerate(zip(before, after)):
             assert a.status == b.status, i

@@ -136,3 +136,22 @@ def test_bf16_matrix_phase_reaches_the_reference_answer(gb, name):
         assert r.bf16_iterations > 0
     else:
         assert r.bf16_iterations == 0
+
+
+def test_problem_autotune_keeps_the_certified_answer(gb):
+    lp, _ = load_lp(os.path.join(GOLD, "rand_cfg0.npz"))
+    opt = gb.Options(precision=gb.Precision.Mixed)
+    p = gb.Problem(lp, opt)
+    try:
+        a = p.solve(opt)
+        t = p.autotune(10)
+        assert 256 <= t["block_nnz"] <= 2048 and 32 <= t["max_rows"] <= 256
+        assert t["ms_per_iter_tuned"] <= 1.05 * t["ms_per_iter_default"]
+        assert t["ms_per_iter_tuned_f64"] <= 1.05 * t["ms_per_iter_default_f64"]
+        assert 256 <= t["block_nnz_f64"] <= 2048
+        b = p.solve(opt)
+        assert a.status == b.status
+        assert max(b.rel_primal, b.rel_dual, b.rel_gap) <= 1e-4 * 1.0000001
+        assert abs(a.pobj - b.pobj) <= 1e-3 * (1 + abs(a.pobj))
+    finally:
+        p.close()
