@@ -81,6 +81,34 @@ class DevBuf {
     size_t n_ = 0;
 };
 
+// Programmatic dependent launch (sm_90+).  A kernel of the iteration loop
+// first lets its successor launch (launch_dependents: the successor's CTAs may
+// be scheduled once every CTA of this grid has started, filling SMs this
+// grid's last wave leaves idle), then waits (wait: blocks until the
+// predecessor grid has completed and its memory is visible) before touching
+// any memory.  Both are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// Launch with the programmatic-stream-serialization attribute (the kernel
+// calls pdl_enter()).
+template <class... KArgs, class... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t s, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    GB_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+}
+
 constexpr int kThreads = 256;  // CTA size of every streaming kernel
 constexpr int kWarps = kThreads / 32;
 

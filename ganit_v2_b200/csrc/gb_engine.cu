@@ -524,11 +524,11 @@ void launch_iteration(Problem& P, VecSet<V>& vs, int k, cudaStream_t s, long lon
     constexpr size_t sm = spmv_smem_bytes<1, V>();
     PrimalArgs<M, V> pa{P.AT.view<M>(), yin, xin, vs.c.get(), vs.l.get(), vs.u.get(),
                         P.has_q ? vs.qx.get() : nullptr, xout, vs.xbar.get(), vs.sumx.get(), P.st.get()};
-    k_primal<M, V><<<pa.AT.nb, kThreads, sm, s>>>(pa);
-    if (mid) GB_CUDA(cudaEventRecord(mid, s));
     DualArgs<M, V> da{P.A.view<M>(), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(),
                       P.st.get()};
-    k_dual<M, V><<<da.A.nb, kThreads, sm, s>>>(da);
+    launch_pdl(k_primal<M, V>, pa.AT.nb, kThreads, sm, s, pa);
+    if (mid) GB_CUDA(cudaEventRecord(mid, s));
+    launch_pdl(k_dual<M, V>, da.A.nb, kThreads, sm, s, da);
     nl += 2;
 }
 
@@ -547,10 +547,10 @@ long long capture_body(Problem& P, int ce, cudaGraphConditionalHandle cond, cuda
     ea.cond = cond;
     ea.use_cond = use_cond;
     const int grid = ea.A.nb + ea.AT.nb;
-    k_eval<M, V, 2, 3><<<grid, kThreads, spmv_smem_bytes<3, V>(), s>>>(ea);
+    launch_pdl(k_eval<M, V, 2, 3>, grid, kThreads, spmv_smem_bytes<3, V>(), s, ea);
     RestartArgs<V> ra{xc, yc, vs.x0.get(), vs.y0.get(), vs.xr.get(), vs.yr.get(), vs.sumx.get(), vs.sumy.get(),
                       P.n, P.m, P.icol(), P.irow(), P.st.get()};
-    k_restart<V><<<elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s>>>(ra);
+    launch_pdl(k_restart<V>, elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s, ra);
     nl += 2;
     return nl;
 }

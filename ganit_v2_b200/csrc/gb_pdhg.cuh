@@ -120,6 +120,7 @@ struct PrimalEpi {
 template <class M, class V>
 __global__ void __launch_bounds__(kThreads, kMinCtas<V>) k_primal(const __grid_constant__ PrimalArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
+    pdl_enter();
     PrimalEpi<M, V> epi{&a, V(0)};
     spmv_run<1, M, V>(a.AT, blockIdx.x, GatherOne<V>{a.y}, epi, smem);
 }
@@ -164,6 +165,7 @@ struct DualEpi {
 template <class M, class V>
 __global__ void __launch_bounds__(kThreads, kMinCtas<V>) k_dual(const __grid_constant__ DualArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
+    pdl_enter();
     DualEpi<M, V> epi{&a, V(0)};
     spmv_run<1, M, V>(a.A, blockIdx.x, GatherOne<V>{a.xbar}, epi, smem);
 }
@@ -436,6 +438,7 @@ static __device__ void decide(SolveState& s, const double (&T)[kTerms], int mode
 template <class M, class V, int NVA, int NVT>
 __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
+    pdl_enter();
     __shared__ double red[kWarps * kTerms];
     __shared__ bool am_last;
     const int nbA = a.A.nb;
@@ -556,6 +559,7 @@ struct RestartArgs {
 
 template <class V>
 __global__ void k_restart(const RestartArgs<V> a) {
+    pdl_enter();
     const bool copy = a.xc != a.x0;
     const int stride = gridDim.x * blockDim.x;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < a.n; j += stride) {
