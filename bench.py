@@ -234,6 +234,37 @@ def run_profile_batch():
     return 0
 
 
+def qp_measure(steps: int = 2) -> dict:
+    """Convex portfolio QP: 100,000 assets, 50-factor risk model, Q = 2(FF^T + D)
+    as the diagonal-plus-low-rank Hessian (workloads.portfolio_qp, seed 7),
+    resident; mixed and FP64 solves to 1e-4, CUDA events on the problem's stream."""
+    import torch
+
+    import ganit_v2_b200 as gb
+    from ganit_v2_b200 import workloads as W
+
+    lp = W.portfolio_qp(100_000, 50, seed=7)
+    out = {"workload": "portfolio QP, 100000 assets x 50 factors, budget row, 0 <= x <= 0.05 (DPLR Hessian)"}
+    for name, prec in (("mixed", gb.Precision.Mixed), ("fp64", gb.Precision.Double)):
+        opt = gb.Options(precision=prec)
+        with gb.Problem(lp, opt) as p:
+            stream = torch.cuda.ExternalStream(p.stream)
+            r = p.solve(opt, fetch=False)
+            ms = []
+            for _ in range(steps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                r = p.solve(opt, fetch=False)
+                e1.record(stream)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+        out[name] = {"solves_per_s": 1e3 / min(ms), "ms": min(ms), "status": r.status_name,
+                     "iterations": r.iterations, "pobj": r.pobj,
+                     "rel_kkt": max(r.rel_primal, r.rel_dual, r.rel_gap)}
+    return out
+
+
 def batch_measure(dist, rank: int, world: int, steps: int = 3, seq_sample: int = 24) -> dict:
     """512 random feasible LPs of log-uniform size (m in [50, 4000],
     n = 2.5 m, 4-12 nonzeros per column, seeds 1000..1511): LPs/s of the
@@ -480,6 +511,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-LP batch measurement")
     ap.add_argument("--no-diff", action="store_true", help="skip the differentiable-layer measurement")
+    ap.add_argument("--no-qp", action="store_true", help="skip the portfolio-QP measurement")
     ap.add_argument("--profile", nargs="?", const="single", choices=["single", "batch"],
                     help="short fixed sequence for ncu: 'single' = the blending LP (upload, two solves, 3 timed "
                          "iterations per level); 'batch' = the 512-LP batch (one solve, 3 timed FP32 iterations)")
@@ -589,6 +621,9 @@ def main():
     diff = None
     if not args.no_diff:
         diff = diff_measure(dist, rank, world)
+    qp = None
+    if not args.no_qp and rank == 0:
+        qp = qp_measure()
     line = None
     if rank == 0:
         cpu = None
@@ -638,6 +673,7 @@ def main():
             "cpu_baseline": cpu,
             "batch": batch,
             "diff": diff,
+            "qp": qp,
         }
         print(json.dumps(line), flush=True)
     prob.close()

@@ -48,9 +48,11 @@ class Status(enum.IntEnum):  # include/ganit/pdhg.hpp:27
     IterationLimit = 2
     TimeLimit = 3
     NumericalError = 4
+    DualInfeasible = 5  # extension (Options.detect_unbounded)
 
 
-STATUS_NAMES = {0: "OPTIMAL", 1: "PRIMAL_INFEASIBLE", 2: "ITERATION_LIMIT", 3: "TIME_LIMIT", 4: "NUMERICAL_ERROR"}
+STATUS_NAMES = {0: "OPTIMAL", 1: "PRIMAL_INFEASIBLE", 2: "ITERATION_LIMIT", 3: "TIME_LIMIT", 4: "NUMERICAL_ERROR",
+                5: "DUAL_INFEASIBLE"}
 
 
 @dataclass
@@ -66,6 +68,7 @@ class Options:  # include/ganit/pdhg.hpp:12-25
     stall_checks: int = 12
     stall_checks_l2: int = 24
     verbose: int = 0
+    detect_unbounded: bool = False  # extension: GB_DUAL_INFEASIBLE from a primal ray (LPs)
 
 
 @dataclass
@@ -109,7 +112,7 @@ class _GbOptions(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iter", C.c_int64), ("time_limit", C.c_double),
                 ("check_every", C.c_int32), ("ruiz_iters", C.c_int32), ("pock_chambolle", C.c_int32),
                 ("infeas_tol", C.c_double), ("precision", C.c_int32), ("stall_checks", C.c_int32),
-                ("stall_checks_l2", C.c_int32), ("verbose", C.c_int32)]
+                ("stall_checks_l2", C.c_int32), ("verbose", C.c_int32), ("detect_unbounded", C.c_int32)]
 
 
 class _GbResult(C.Structure):
@@ -250,7 +253,8 @@ class _LpView:
 def _opts(opt: Options | None) -> _GbOptions:
     o = opt or Options()
     return _GbOptions(o.tol, o.max_iter, o.time_limit, o.check_every, o.ruiz_iters, int(o.pock_chambolle),
-                      o.infeas_tol, int(o.precision), o.stall_checks, o.stall_checks_l2, int(o.verbose))
+                      o.infeas_tol, int(o.precision), o.stall_checks, o.stall_checks_l2, int(o.verbose),
+                      int(bool(o.detect_unbounded)))
 
 
 def _result(r: _GbResult, x, y) -> Result:

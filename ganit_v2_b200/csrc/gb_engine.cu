@@ -198,6 +198,10 @@ void init_kernel_attrs() {
         set_smem(k_eval<float, float, 2, 3>, spmv_smem_bytes<3, float>());
         set_smem(k_eval<float, double, 2, 3>, spmv_smem_bytes<3, double>());
         set_smem(k_eval<double, double, 2, 3>, spmv_smem_bytes<3, double>());
+        // checks that also form A (x - x_r) for the unbounded test
+        set_smem(k_eval<float, float, 3, 3>, spmv_smem_bytes<3, float>());
+        set_smem(k_eval<float, double, 3, 3>, spmv_smem_bytes<3, double>());
+        set_smem(k_eval<double, double, 3, 3>, spmv_smem_bytes<3, double>());
         set_smem(k_spmv_q2<float, double>, spmv_smem_bytes<2, double>());
         set_smem(k_spmv_q2<double, double>, spmv_smem_bytes<2, double>());
     });
@@ -547,7 +551,10 @@ long long capture_body(Problem& P, int ce, cudaGraphConditionalHandle cond, cuda
     ea.cond = cond;
     ea.use_cond = use_cond;
     const int grid = ea.A.nb + ea.AT.nb;
-    launch_pdl(k_eval<M, V, 2, 3>, grid, kThreads, spmv_smem_bytes<3, V>(), s, ea);
+    if (P.detect_unbounded && !P.has_q)  // third right-hand side of the A pass: the primal ray
+        launch_pdl(k_eval<M, V, 3, 3>, grid, kThreads, spmv_smem_bytes<3, V>(), s, ea);
+    else
+        launch_pdl(k_eval<M, V, 2, 3>, grid, kThreads, spmv_smem_bytes<3, V>(), s, ea);
     RestartArgs<V> ra{xc, yc, vs.x0.get(), vs.y0.get(), vs.xr.get(), vs.yr.get(), vs.sumx.get(), vs.sumy.get(),
                       P.n, P.m, P.icol(), P.irow(), P.st.get()};
     launch_pdl(k_restart<V>, elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s, ra);
@@ -559,10 +566,12 @@ template <class M, class V>
 LevelGraph* level_graph(Problem& P, int ce) {
     constexpr int li = level_index<M, V>();
     auto& slot = P.graphs[li];
-    if (slot && slot->check_every == ce) return slot.get();
+    const int ray = P.detect_unbounded && !P.has_q ? 1 : 0;
+    if (slot && slot->check_every == ce && slot->ray == ray) return slot.get();
     slot.reset(new LevelGraph);
     LevelGraph* g = slot.get();
     g->check_every = ce;
+    g->ray = ray;
     GB_CUDA(cudaGraphCreate(&g->graph, 0));
     cudaGraphConditionalHandle h;
     GB_CUDA(cudaGraphConditionalHandleCreate(&h, g->graph, 1, cudaGraphCondAssignDefault));
@@ -581,9 +590,16 @@ LevelGraph* level_graph(Problem& P, int ce) {
     try {
         nl = capture_body<M, V>(P, ce, h, cs);
     } catch (...) {
-        cudaGraph_t dummy;
+        // A failed launch invalidated the capture: end it, and drop this
+        // LevelGraph without tearing down its half-built graph (a handle is
+        // leaked on this error path rather than destroyed in an unknown state).
+        cudaGraph_t dummy = nullptr;
         cudaStreamEndCapture(cs, &dummy);
+        cudaGetLastError();
         cudaStreamDestroy(cs);
+        g->graph = nullptr;
+        g->exec = nullptr;
+        slot.reset();
         throw;
     }
     GB_CUDA(cudaStreamEndCapture(cs, &body));
@@ -621,7 +637,7 @@ __global__ void k_set_phase(int count, SolveState* st, const int* flags, double 
 }
 
 __global__ void k_init_state(int count, SolveState* st, const double* sc, int has_q, int check_every,
-                             long long max_iter, double time_limit, double infeas_tol) {
+                             long long max_iter, double time_limit, double infeas_tol, int detect_unbounded) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= count) return;
     const double* s0 = sc + static_cast<size_t>(k) * kScal;
@@ -640,6 +656,7 @@ __global__ void k_init_state(int count, SolveState* st, const double* sc, int ha
     s.max_iter = max_iter;
     s.check_every = check_every;
     s.has_q = has_q;
+    s.detect_unbounded = detect_unbounded;
     s.carry_restart_err = -1.0;
     s.restart_err = -1.0;
     s.t0_ns = global_ns();
@@ -725,6 +742,7 @@ int status_from(int e) {  // pdhg_impl.hpp:232-240
     switch (e) {
         case kConverged: return GB_OPTIMAL;
         case kInfeasible: return GB_PRIMAL_INFEASIBLE;
+        case kUnbounded: return GB_DUAL_INFEASIBLE;
         case kTimeLimit: return GB_TIME_LIMIT;
         case kNumerical: return GB_NUMERICAL_ERROR;
         default: return GB_ITERATION_LIMIT;
@@ -740,9 +758,10 @@ void solve_problem(Problem& P, const gb_options* opt, gb_result* res) {
     const auto t0 = std::chrono::steady_clock::now();
     const int K = P.count;
     P.launches = 0;
+    P.detect_unbounded = opt->detect_unbounded != 0;
     k_init_state<<<div_up(K, kThreads), kThreads, 0, s>>>(K, P.st.get(), P.scal.get(), P.has_q ? 1 : 0,
                                                           opt->check_every, opt->max_iter, opt->time_limit,
-                                                          opt->infeas_tol);
+                                                          opt->infeas_tol, P.detect_unbounded ? 1 : 0);
     k_start_point<<<elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s>>>(P.n, P.m, P.l.get(), P.u.get(),
                                                                          P.x64.get(), P.y64.get());
     P.launches += 2;
@@ -767,7 +786,7 @@ void solve_problem(Problem& P, const gb_options* opt, gb_result* res) {
             if (!P.phase_flags_host[k] || done[k]) continue;
             const int e = ex[k];
             done[k] = (e == kConverged && kkt_conv_h(P.st_host[k].kcert, opt->tol)) || e == kTimeLimit ||
-                      e == kIterLimit || e == kInfeasible;
+                      e == kIterLimit || e == kInfeasible || e == kUnbounded;
         }
     };
     if (opt->precision != GB_PREC_DOUBLE) {
@@ -1036,6 +1055,7 @@ void gb_default_options(gb_options* o) {
     o->stall_checks = 12;
     o->stall_checks_l2 = 24;
     o->verbose = 0;
+    o->detect_unbounded = 0;
 }
 
 int gb_set_device(int device) {

@@ -32,7 +32,10 @@ struct Kkt {
 };
 
 // Phase exits (pdhg_impl.hpp:65)
-enum PhaseExit : int { kConverged = 0, kStalled = 1, kIterLimit = 2, kTimeLimit = 3, kInfeasible = 4, kNumerical = 5 };
+enum PhaseExit : int {
+    kConverged = 0, kStalled = 1, kIterLimit = 2, kTimeLimit = 3, kInfeasible = 4, kNumerical = 5,
+    kUnbounded = 6  // extension: primal ray certificate of dual infeasibility
+};
 enum EvalMode : int { kEvalInit = 0, kEvalCheck = 1, kEvalCertify = 2 };
 
 // Device-resident solver state of one instance (PdhgShared + PdhgState + loop
@@ -62,7 +65,7 @@ struct alignas(16) SolveState {
     int active;                // iterating in the current phase
     int in_phase;              // took part in the current phase
     int ran_body;              // iterated during the body that ended at the last check
-    int pad_;
+    int detect_unbounded;      // test the primal ray (extension, LPs)
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -175,6 +178,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtas<V>) k_dual(const __grid_con
 enum Term : int {
     T_RP2_C = 0, T_RP2_A, T_ROBJ_C, T_ROBJ_A, T_ROBJ_R, T_DY2_C, T_DY2_A,
     T_RD2_C, T_VOBJ_C, T_RD2_A, T_VOBJ_A, T_RD2_R, T_VOBJ_R, T_CX_C, T_CX_A, T_XQX_C, T_XQX_A, T_DX2_C, T_DX2_A,
+    T_UR2, T_UC2, T_CD,  // primal ray d = x - x_r: row / column recession violations^2, c'd
     kTerms
 };
 
@@ -214,13 +218,16 @@ __device__ __forceinline__ V avg_of(const V* s, int k, double inv) {
 }
 
 template <class V, int NV>
-struct GatherXAvg {  // A side: x and (check) the running average xa
+struct GatherXAvg {  // A side: x, (check) the running average xa, (unbounded test) the ray x - xr
     const V* __restrict__ x;
     const V* __restrict__ sumx;
+    const V* __restrict__ xr;
     double inv;
     __device__ __forceinline__ void operator()(int j, V (&o)[NV]) const {
-        o[0] = __ldg(x + j);
+        const V xj = __ldg(x + j);
+        o[0] = xj;
         if (NV > 1) o[NV > 1 ? 1 : 0] = avg_of(sumx, j, inv);
+        if (NV > 2) o[NV > 2 ? 2 : 0] = xj - __ldg(xr + j);
     }
 };
 
@@ -285,6 +292,14 @@ struct EvalRowEpi {
             t[T_DY2_C] += d0 * d0;
             t[T_DY2_A] += d1 * d1;
         }
+        if (NV > 2) {  // A d must lie in the row's recession cone: >= 0 if lo finite, <= 0 if hi finite
+            const double ad = double(s[NV > 2 ? 2 : 0]);
+            double v = 0.0;
+            if (isfinite(lo) && ad < 0) v -= ad;
+            if (isfinite(hi) && ad > 0) v += ad;
+            v /= r;
+            t[T_UR2] += v * v;
+        }
     }
 };
 
@@ -322,6 +337,10 @@ struct EvalColEpi {
             const double d0 = double(xj) - double(xrj), d1 = double(xa) - double(xrj);
             t[T_DX2_C] += d0 * d0;
             t[T_DX2_A] += d1 * d1;
+            // the ray within the column's recession cone: >= 0 if l finite, <= 0 if u finite
+            const double vc = (isfinite(lj) && d0 < 0 ? -d0 : 0.0) + (isfinite(uj) && d0 > 0 ? d0 : 0.0);
+            t[T_UC2] += vc * vc;
+            t[T_CD] += cj * d0;
         }
     }
 };
@@ -401,7 +420,14 @@ static __device__ void decide(SolveState& s, const double (&T)[kTerms], int mode
             const double dray = (T[T_ROBJ_R] + T[T_VOBJ_R]) * s.obj_scale;
             infeasible = (dray > 0) && sqrt(T[T_RD2_R]) * (1.0 + s.bnorm) / dray <= s.infeas_tol;
         }
+        bool unbounded = false;
+        if (!infeasible && s.detect_unbounded && !s.has_q && it_since >= 4LL * s.check_every) {
+            // extension: dual infeasibility from the primal ray d = x - x_r
+            const double cd = T[T_CD];
+            unbounded = cd < 0 && T[T_DX2_C] > 1e-20 && sqrt(T[T_UR2] + T[T_UC2]) / (-cd) <= s.infeas_tol;
+        }
         if (infeasible) { s.exit_reason = kInfeasible; s.best = kcand; s.best_is_avg = avg_better; }
+        else if (unbounded) { s.exit_reason = kUnbounded; s.best = kcand; s.best_is_avg = avg_better; }
         else {
             done = 0;
             if (kcand.err < 0.8 * s.best_err) { s.best_err = kcand.err; s.cwp = 0; }
@@ -448,7 +474,7 @@ __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalA
         EvalRowEpi<M, V, NVA> epi{a, inv, {}};
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) epi.t[k] = 0.0;
-        spmv_run<NVA, M, V>(a.A, blockIdx.x, GatherXAvg<V, NVA>{a.x, a.sumx, inv}, epi, smem);
+        spmv_run<NVA, M, V>(a.A, blockIdx.x, GatherXAvg<V, NVA>{a.x, a.sumx, a.xr, inv}, epi, smem);
 #pragma unroll
         for (int k = 0; k < kTerms; ++k) t[k] = epi.t[k];
     } else {

@@ -78,6 +78,7 @@ struct LevelGraph {
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
     int check_every = 0;
+    int ray = 0;  // the check also forms A (x - x_r) (unbounded test)
     long long launches_per_body = 0;
     ~LevelGraph() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -127,6 +128,7 @@ struct Problem {
     long long launches = 0;               // kernel launches of the last solve
     std::vector<InstanceResult> results;
     bool solved = false;
+    bool detect_unbounded = false;        // option of the current solve (LPs)
     // row-split schedule tunables per instance and schedule (index 0: FP32 /
     // BF16 kernels, 1: FP64 kernels); set by the autotuner
     std::vector<int> tune_block_nnz[2], tune_max_rows[2];

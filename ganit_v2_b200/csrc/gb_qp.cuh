@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_q2(const __grid_constant__ Cs
     extern __shared__ __align__(16) unsigned char smem[];
     const double inv = 1.0 / static_cast<double>(st->it_since + st->check_every);
     Store2Epi<V> epi{qx, qxa};
-    spmv_run<2, M, V>(Q, blockIdx.x, GatherXAvg<V, 2>{x, sumx, inv}, epi, smem);
+    spmv_run<2, M, V>(Q, blockIdx.x, GatherXAvg<V, 2>{x, sumx, nullptr, inv}, epi, smem);
 }
 
 // Partial F^T v for NV vectors: v0 = x, v1 = inv * sumx (when NV == 2).

@@ -328,6 +328,31 @@ def diff_batch(count: int = 256, m: int = 500, n: int = 1000, nnz_per_col: int =
     return [nondegenerate_lp(m, n, nnz_per_col, seed=seed + i, max_cond=max_cond) for i in range(count)]
 
 
+def unbounded_lp(m: int = 200, n: int = 500, nnz_per_col: int = 6, seed: int = 4) -> LP:
+    """Feasible LP with an unbounded objective (dual infeasible).
+
+    A :func:`random_feasible_lp` plus two columns ``a`` and ``-a`` (a random
+    sparse column), both in ``[0, inf)`` with costs ``(-1, 0)``: the ray
+    ``d = e_{n} + e_{n+1}`` keeps ``A x`` fixed, stays in the bounds and
+    lowers the objective without limit, while x0 (extended by zeros) stays
+    feasible.  ``meta['ray']`` holds d."""
+    base = random_feasible_lp(m, n, nnz_per_col, seed=seed)
+    rng = np.random.default_rng(seed + 7919)
+    A = base.A.to_scipy().tocsc()
+    rows = rng.choice(m, size=min(nnz_per_col, m), replace=False)
+    vals = rng.standard_normal(rows.shape[0])
+    col = sp.csc_matrix((vals, (rows, np.zeros_like(rows))), shape=(m, 1))
+    A2 = sp.hstack([A, col, -col], format="csr")
+    A2.sort_indices()
+    c = np.concatenate([base.c, [-1.0, 0.0]])
+    l = np.concatenate([base.l, [0.0, 0.0]])
+    u = np.concatenate([base.u, [np.inf, np.inf]])
+    ray = np.zeros(n + 2)
+    ray[n] = ray[n + 1] = 1.0
+    return LP(Csr.from_scipy(A2), c, l, u, base.lo, base.hi, name=f"unbounded_m{m}_n{n}_s{seed}",
+              meta={"x0": np.concatenate([base.meta["x0"], [0.0, 0.0]]), "ray": ray})
+
+
 def infeasible_lp(m: int = 200, n: int = 500, seed: int = 3) -> LP:
     """A random feasible LP made primal infeasible by two contradicting rows
     ``a'x <= b - 1`` and ``a'x >= b`` on the same random row vector a."""

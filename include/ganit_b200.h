@@ -46,7 +46,11 @@ enum {
 };
 
 /* ---- solver status, include/ganit/pdhg.hpp:27 (same order) */
-enum { GB_OPTIMAL = 0, GB_PRIMAL_INFEASIBLE = 1, GB_ITERATION_LIMIT = 2, GB_TIME_LIMIT = 3, GB_NUMERICAL_ERROR = 4 };
+enum { GB_OPTIMAL = 0, GB_PRIMAL_INFEASIBLE = 1, GB_ITERATION_LIMIT = 2, GB_TIME_LIMIT = 3, GB_NUMERICAL_ERROR = 4,
+       /* extension (gb_options.detect_unbounded): a primal ray certifies that
+        * the LP is unbounded (its dual infeasible); the reference has no such
+        * test and reports ITERATION_LIMIT or TIME_LIMIT there (README.md:197) */
+       GB_DUAL_INFEASIBLE = 5 };
 
 /* ---- precision schedule, include/ganit/pdhg.hpp:10 (same order) */
 enum { GB_PREC_DOUBLE = 0, GB_PREC_MIXED = 1, GB_PREC_DYNAMIC = 2,
@@ -97,6 +101,12 @@ typedef struct {
     int32_t stall_checks;    /* 12 */
     int32_t stall_checks_l2; /* 24 */
     int32_t verbose;         /* 0 (the engine prints nothing) */
+    /* Extension, off by default (as the reference): test the primal ray
+     * d = x - x_r every check once 4 checks have passed since the last
+     * restart, and stop with GB_DUAL_INFEASIBLE when c'd < 0 and the
+     * violation of d's recession conditions (A d within the rows' recession
+     * cones, d within the bounds') divided by -c'd is <= infeas_tol.  LPs. */
+    int32_t detect_unbounded;
 } gb_options;
 
 /* ganit::Result (include/ganit/pdhg.hpp:30-42) without the vectors, which go

@@ -93,3 +93,13 @@ def test_diff_batch_is_deterministic_and_conditioned():
         A = lp.A.to_scipy().tocsr()
         B = A[np.flatnonzero(lp.meta["tight"])][:, np.flatnonzero(lp.meta["interior"])].toarray()
         assert np.linalg.cond(B, 1) <= 1e4 * 1.0001
+
+
+def test_unbounded_lp_has_an_improving_recession_ray():
+    lp = W.unbounded_lp(60, 150, 5, seed=2)
+    A = lp.A.to_scipy().tocsr()
+    d, x0 = lp.meta["ray"], lp.meta["x0"]
+    assert np.allclose(A @ d, 0.0) and lp.c @ d < 0
+    assert np.all(d[np.isfinite(lp.l)] >= 0) and np.all(d[np.isfinite(lp.u)] == 0)
+    ax = A @ x0
+    assert np.all(ax <= lp.hi + 1e-9) and np.all(ax[np.isfinite(lp.lo)] >= lp.lo[np.isfinite(lp.lo)] - 1e-9)
