@@ -19,7 +19,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .lp import LP
+from .lp import LP, Csr
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libganit_b200.so")
@@ -162,7 +162,7 @@ EXPORTS = [
     "gb_batch_get_solution", "gb_batch_schedule", "gb_batch_autotune", "gb_batch_time_kernels", "gb_batch_destroy",
     "gb_diff_create", "gb_diff_forward",
     "gb_diff_default_options", "gb_diff_set_options", "gb_diff_backward", "gb_diff_get_info", "gb_diff_tail_start", "gb_diff_destroy",
-    "gb_eval_kkt_noalloc",
+    "gb_eval_kkt_noalloc", "gb_read_mps", "gb_model_lp", "gb_model_name", "gb_model_free",
 ]
 
 _lib = None
@@ -204,6 +204,8 @@ def load_library(path: str = LIB_PATH):
         "gb_diff_backward": (i32, [vp, vp, vp, vp, vp, vp, vp]), "gb_diff_get_info": (i32, [vp, i32, vp]),
         "gb_diff_tail_start": (i32, [vp, vp, vp]), "gb_diff_destroy": (None, [vp]),
         "gb_eval_kkt_noalloc": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
+        "gb_read_mps": (i32, [C.c_char_p, vp]), "gb_model_lp": (vp, [vp]), "gb_model_name": (C.c_char_p, [vp]),
+        "gb_model_free": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -261,6 +263,37 @@ def _result(r: _GbResult, x, y) -> Result:
     return Result(Status(r.status), x, y, r.pobj, r.dobj, r.rel_primal, r.rel_dual, r.rel_gap, r.iterations,
                   r.fp32_iterations, r.l2_iterations, r.restarts, r.setup_seconds, r.solve_seconds, "b200",
                   r.norm_a, r.primal_weight, r.checks, r.phases, r.bf16_iterations)
+
+
+def read_mps(path: str) -> LP:
+    """Read an MPS / QPS file with the library's reader (gb_read_mps; the
+    format rules of the reference's src/mps.cpp:69-272).  No GPU needed."""
+    lib = load_library()
+    h = C.c_void_p()
+    _check(lib.gb_read_mps(os.fsencode(path), C.byref(h)))
+    try:
+        v = _GbLp.from_address(lib.gb_model_lp(h))
+        m, n = v.m, v.n
+
+        def arr(ptr, k, dt):
+            if not ptr or k == 0:
+                return np.zeros(k, dtype=dt)
+            ct = C.c_int32 if dt == np.int32 else C.c_double
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(k,)).astype(dt, copy=True)
+
+        ptr = arr(v.a_ptr, m + 1, np.int32)
+        nnz = int(ptr[-1]) if m else 0
+        A = Csr(m, n, ptr, arr(v.a_idx, nnz, np.int32), arr(v.a_val, nnz, np.float64))
+        Q = None
+        if v.q_ptr:
+            qp = arr(v.q_ptr, n + 1, np.int32)
+            Q = Csr(n, n, qp, arr(v.q_idx, int(qp[-1]), np.int32), arr(v.q_val, int(qp[-1]), np.float64))
+        name = lib.gb_model_name(h).decode(errors="replace") or os.path.basename(path)
+        return LP(A, arr(v.c, n, np.float64), arr(v.l, n, np.float64), arr(v.u, n, np.float64),
+                  arr(v.lo, m, np.float64), arr(v.hi, m, np.float64), obj_const=float(v.obj_const),
+                  maximize=bool(v.maximize), Q=Q, name=name)
+    finally:
+        lib.gb_model_free(h)
 
 
 def release_cached_memory() -> None:

@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libganit_b200.so")
-SOURCES = ["gb_engine.cu", "gb_backend.cu", "gb_diff.cu", "gb_noalloc.cu", "gb_pool.cu"]
+SOURCES = ["gb_engine.cu", "gb_backend.cu", "gb_diff.cu", "gb_noalloc.cu", "gb_pool.cu", "gb_mps.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]
@@ -46,7 +46,7 @@ def build(force: bool = False, verbose: bool = False, jobs: int = 4) -> str:
     cc = nvcc()
     procs, objs = [], []
     for src in SOURCES:
-        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
         objs.append(obj)
         cmd = [cc, *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:

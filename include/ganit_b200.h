@@ -304,6 +304,18 @@ int gb_batch_time_kernels(gb_batch* b, int level, int iters, double* ms_primal, 
                           double* bytes_per_iter);
 void gb_batch_destroy(gb_batch* b);
 
+/* ---------------------------------------------------------------- 3c. problem files
+ * Replaces ganit::read_mps (src/mps.cpp:69-272) for callers that feed the
+ * engine directly from an MPS / QPS file, with the same format rules
+ * (sections, N rows, RHS / RANGES / BOUNDS semantics, QUADOBJ mirrored,
+ * integrality markers ignored).  gb_model_lp returns a view of the model,
+ * valid until gb_model_free, that gb_solve / gb_problem_create accept. */
+typedef struct gb_model gb_model;
+int gb_read_mps(const char* path, gb_model** out);
+const gb_lp* gb_model_lp(const gb_model* model);
+const char* gb_model_name(const gb_model* model);
+void gb_model_free(gb_model* model);
+
 /* ---------------------------------------------------------------- 3b. differentiable solving
  * No counterpart in the reference (it differentiates run_pdhg,
  * src/pdhg_impl.hpp:243-328).  LPs only.

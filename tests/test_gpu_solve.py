@@ -155,3 +155,58 @@ def test_problem_autotune_keeps_the_certified_answer(gb):
         assert abs(a.pobj - b.pobj) <= 1e-3 * (1 + abs(a.pobj))
     finally:
         p.close()
+
+
+def _write_mps(lp, path):
+    """Free-format MPS of an LP (row bounds as E / L / G rows with ranges)."""
+    A = lp.A.to_scipy().tocsc()
+    lines = ["NAME TEST", "ROWS", " N OBJ"]
+    kind, rhs, rng = [], [], []
+    for i in range(lp.m):
+        lo, hi = lp.lo[i], lp.hi[i]
+        if lo == hi:
+            kind.append("E"); rhs.append(lo); rng.append(None)
+        elif np.isinf(lo):
+            kind.append("L"); rhs.append(hi); rng.append(None)
+        elif np.isinf(hi):
+            kind.append("G"); rhs.append(lo); rng.append(None)
+        else:
+            kind.append("G"); rhs.append(lo); rng.append(hi - lo)
+        lines.append(f" {kind[-1]} R{i}")
+    lines.append("COLUMNS")
+    for j in range(lp.n):
+        lines.append(f"    C{j} OBJ {float(lp.c[j])!r}")
+        for p in range(A.indptr[j], A.indptr[j + 1]):
+            lines.append(f"    C{j} R{A.indices[p]} {float(A.data[p])!r}")
+    lines.append("RHS")
+    lines += [f"    RHS R{i} {float(rhs[i])!r}" for i in range(lp.m) if rhs[i] != 0]
+    lines.append("RANGES")
+    lines += [f"    RNG R{i} {float(rng[i])!r}" for i in range(lp.m) if rng[i] is not None]
+    lines.append("BOUNDS")
+    for j in range(lp.n):
+        l, u = lp.l[j], lp.u[j]
+        if np.isinf(l) and np.isinf(u):
+            lines.append(f" FR BND C{j}")
+            continue
+        if np.isinf(l):
+            lines.append(f" MI BND C{j}")
+        elif l != 0:
+            lines.append(f" LO BND C{j} {float(l)!r}")
+        if not np.isinf(u):
+            lines.append(f" UP BND C{j} {float(u)!r}")
+    lines.append("ENDATA")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def test_problem_read_from_an_mps_file_solves_like_the_in_memory_one(gb, tmp_path):
+    lp, _ = load_lp(os.path.join(GOLD, "rand_small.npz"))
+    path = str(tmp_path / "rand_small.mps")
+    _write_mps(lp, path)
+    fl = gb.read_mps(path)
+    opt = gb.Options(precision=gb.Precision.Double)
+    a = gb.solve_pdhg_gpu(lp, opt)
+    b = gb.solve_pdhg_gpu(fl, opt)
+    assert a.status == b.status and a.iterations == b.iterations
+    np.testing.assert_array_equal(a.x, b.x)
+    np.testing.assert_array_equal(a.y, b.y)
