@@ -155,7 +155,8 @@ class GbKkt(C.Structure):
 EXPORTS = [
     "gb_last_error", "gb_release_cached_memory", "gb_cached_memory_bytes", "gb_version", "gb_default_options", "gb_set_device", "gb_solve", "gb_problem_create",
     "gb_problem_solve", "gb_problem_get_solution", "gb_problem_destroy", "gb_problem_stream",
-    "gb_problem_time_kernels", "gb_problem_stats", "gb_problem_autotune", "gb_backend_create", "gb_backend_destroy", "gb_vec_zeros",
+    "gb_problem_time_kernels", "gb_problem_stats", "gb_problem_autotune", "gb_problem_time_kernels_graph",
+    "gb_batch_time_kernels_graph", "gb_backend_create", "gb_backend_destroy", "gb_vec_zeros",
     "gb_vec_from_host", "gb_vec_to_host", "gb_vec_size", "gb_vec_destroy", "gb_copy", "gb_fill", "gb_spmv_A",
     "gb_spmv_AT", "gb_spmv_Q", "gb_primal_step", "gb_dual_step", "gb_sub", "gb_scale_into", "gb_primal_res2",
     "gb_dual_res", "gb_row_dual_obj", "gb_dot", "gb_dot_c", "gb_diff2", "gb_batch_create", "gb_batch_solve",
@@ -184,7 +185,9 @@ def load_library(path: str = LIB_PATH):
         "gb_problem_create": (i32, [vp, vp, vp]), "gb_problem_solve": (i32, [vp, vp, vp]),
         "gb_problem_get_solution": (i32, [vp, vp, vp]), "gb_problem_destroy": (None, [vp]),
         "gb_problem_stream": (vp, [vp]), "gb_problem_time_kernels": (i32, [vp, i32, i32, vp, vp, vp]),
-        "gb_problem_stats": (i32, [vp, vp, vp]), "gb_problem_autotune": (i32, [vp, i32, vp, vp, vp, vp]), "gb_backend_create": (i32, [vp, i32, i32, vp]),
+        "gb_problem_stats": (i32, [vp, vp, vp]), "gb_problem_autotune": (i32, [vp, i32, vp, vp, vp, vp]),
+        "gb_problem_time_kernels_graph": (i32, [vp, i32, i32, vp, vp, vp]),
+        "gb_batch_time_kernels_graph": (i32, [vp, i32, i32, vp, vp, vp]), "gb_backend_create": (i32, [vp, i32, i32, vp]),
         "gb_backend_destroy": (None, [vp]), "gb_vec_zeros": (i32, [vp, i32, vp]),
         "gb_vec_from_host": (i32, [vp, vp, i32, vp]), "gb_vec_to_host": (i32, [vp, vp, vp]),
         "gb_vec_size": (i32, [vp]), "gb_vec_destroy": (None, [vp]), "gb_copy": (i32, [vp, vp, vp]),
@@ -371,6 +374,13 @@ class Problem:
                 "ms_per_iter_tuned": float(t1[0]), "block_nnz_f64": int(bn[1]), "max_rows_f64": int(mr[1]),
                 "ms_per_iter_default_f64": float(t0[1]), "ms_per_iter_tuned_f64": float(t1[1])}
 
+    def time_kernels_graph(self, level: int, iters: int = 200) -> dict:
+        """Back-to-back launches captured in CUDA graphs (gb_problem_time_kernels_graph)."""
+        mp, md, mi = C.c_double(), C.c_double(), C.c_double()
+        _check(self._lib.gb_problem_time_kernels_graph(self._h, int(level), int(iters), C.byref(mp), C.byref(md),
+                                                       C.byref(mi)))
+        return {"ms_primal": mp.value, "ms_dual": md.value, "ms_iteration": mi.value}
+
     def stats(self):
         nl = C.c_int64()
         bpi = np.zeros(3)
@@ -463,6 +473,13 @@ class BatchSolver:
         _check(self._lib.gb_batch_time_kernels(self._h, int(level), int(iters), C.byref(mp), C.byref(md),
                                                C.byref(nl), C.byref(bpi)))
         return {"ms_primal": mp.value, "ms_dual": md.value, "launches": nl.value, "bytes_per_iter": bpi.value}
+
+    def time_kernels_graph(self, level: int = 0, iters: int = 100) -> dict:
+        """Back-to-back launches captured in CUDA graphs (gb_batch_time_kernels_graph)."""
+        mp, md, mi = C.c_double(), C.c_double(), C.c_double()
+        _check(self._lib.gb_batch_time_kernels_graph(self._h, int(level), int(iters), C.byref(mp), C.byref(md),
+                                                     C.byref(mi)))
+        return {"ms_primal": mp.value, "ms_dual": md.value, "ms_iteration": mi.value}
 
     def close(self):
         if getattr(self, "_h", None):

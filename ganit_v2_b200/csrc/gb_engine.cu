@@ -517,19 +517,27 @@ EvalArgs<M, V> eval_args(Problem& P, VecSet<V>& vs, const V* x, const V* y, int 
     return a;
 }
 
-// One PDHG iteration (k-th inside the body) on buffers selected by parity.
+// Arguments of the two kernels of the k-th iteration inside a body (buffers by parity).
 template <class M, class V>
-void launch_iteration(Problem& P, VecSet<V>& vs, int k, cudaStream_t s, long long& nl, cudaEvent_t mid = nullptr) {
+void iteration_args(Problem& P, VecSet<V>& vs, int k, PrimalArgs<M, V>& pa, DualArgs<M, V>& da) {
     const V* xin = (k & 1) ? vs.x1.get() : vs.x0.get();
     V* xout = (k & 1) ? vs.x0.get() : vs.x1.get();
     const V* yin = (k & 1) ? vs.y1.get() : vs.y0.get();
     V* yout = (k & 1) ? vs.y0.get() : vs.y1.get();
-    if (P.has_q) launch_qx<M, V>(P, vs, xin, vs.qx.get(), s, nl);
+    pa = PrimalArgs<M, V>{P.AT.view<M>(), yin, xin, vs.c.get(), vs.l.get(), vs.u.get(),
+                          P.has_q ? vs.qx.get() : nullptr, xout, vs.xbar.get(), vs.sumx.get(), P.st.get()};
+    da = DualArgs<M, V>{P.A.view<M>(), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(),
+                        P.st.get()};
+}
+
+// One PDHG iteration (k-th inside the body) on buffers selected by parity.
+template <class M, class V>
+void launch_iteration(Problem& P, VecSet<V>& vs, int k, cudaStream_t s, long long& nl, cudaEvent_t mid = nullptr) {
+    PrimalArgs<M, V> pa;
+    DualArgs<M, V> da;
+    iteration_args<M, V>(P, vs, k, pa, da);
+    if (P.has_q) launch_qx<M, V>(P, vs, pa.x, vs.qx.get(), s, nl);
     constexpr size_t sm = spmv_smem_bytes<1, V>();
-    PrimalArgs<M, V> pa{P.AT.view<M>(), yin, xin, vs.c.get(), vs.l.get(), vs.u.get(),
-                        P.has_q ? vs.qx.get() : nullptr, xout, vs.xbar.get(), vs.sumx.get(), P.st.get()};
-    DualArgs<M, V> da{P.A.view<M>(), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(),
-                      P.st.get()};
     launch_pdl(k_primal<M, V>, pa.AT.nb, kThreads, sm, s, pa);
     if (mid) GB_CUDA(cudaEventRecord(mid, s));
     launch_pdl(k_dual<M, V>, da.A.nb, kThreads, sm, s, da);
@@ -863,6 +871,12 @@ void solve_problem(Problem& P, const gb_options* opt, gb_result* res) {
 }
 
 // ---------------------------------------------------------------- kernel timing
+template <class M_, class V_>
+struct Tag {
+    using M = M_;
+    using V = V_;
+};
+
 template <class M, class V>
 void time_level(Problem& P, int iters, double* msp, double* msd, int64_t* launches) {
     cudaStream_t s = P.stream;
@@ -893,6 +907,81 @@ void time_level(Problem& P, int iters, double* msp, double* msd, int64_t* launch
     *msp = tp / iters;
     *msd = td / iters;
     *launches = nl;
+}
+
+// Average device time of k_primal and of k_dual when launched back to back
+// (each captured `iters` times into a CUDA graph with programmatic dependent
+// launch, as the solve loop issues them, and the graph timed with two CUDA
+// events), and of one full iteration (the pair, alternating buffers).  Every
+// instance is active.  Warm L2: the same matrix and vectors every launch.
+template <class M, class V>
+void time_level_graph(Problem& P, int iters, double* msp, double* msd, double* msi) {
+    cudaStream_t s = P.stream;
+    VecSet<V>& vs = Level<M, V>::vs(P);
+    k_activate_all<<<div_up(P.count, kThreads), kThreads, 0, s>>>(P.count, P.st.get());
+    k_phase_in<V><<<elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s>>>(
+        P.n, P.m, P.icol(), P.irow(), P.st.get(), P.x64.get(), P.y64.get(), P.x64.get(), P.y64.get(), 0,
+        vs.x0.get(), vs.y0.get(), vs.xr.get(), vs.yr.get(), vs.sumx.get(), vs.sumy.get());
+    PrimalArgs<M, V> pa;
+    DualArgs<M, V> da;
+    iteration_args<M, V>(P, vs, 0, pa, da);
+    constexpr size_t sm = spmv_smem_bytes<1, V>();
+    auto timed_graph = [&](auto&& body) {
+        cudaStream_t cs;
+        GB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ge = nullptr;
+        GB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        try {
+            body(cs);
+        } catch (...) {
+            cudaStreamEndCapture(cs, &g);
+            cudaGetLastError();
+            cudaStreamDestroy(cs);
+            throw;
+        }
+        GB_CUDA(cudaStreamEndCapture(cs, &g));
+        GB_CUDA(cudaStreamDestroy(cs));
+        GB_CUDA(cudaGraphInstantiate(&ge, g, 0));
+        cudaEvent_t e0, e1;
+        GB_CUDA(cudaEventCreate(&e0));
+        GB_CUDA(cudaEventCreate(&e1));
+        GB_CUDA(cudaGraphLaunch(ge, s));  // warm-up
+        GB_CUDA(cudaEventRecord(e0, s));
+        GB_CUDA(cudaGraphLaunch(ge, s));
+        GB_CUDA(cudaEventRecord(e1, s));
+        GB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        GB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaGraphExecDestroy(ge);
+        cudaGraphDestroy(g);
+        return static_cast<double>(ms) / iters;
+    };
+    *msp = timed_graph([&](cudaStream_t cs) {
+        for (int k = 0; k < iters; ++k) launch_pdl(k_primal<M, V>, pa.AT.nb, kThreads, sm, cs, pa);
+    });
+    *msd = timed_graph([&](cudaStream_t cs) {
+        for (int k = 0; k < iters; ++k) launch_pdl(k_dual<M, V>, da.A.nb, kThreads, sm, cs, da);
+    });
+    *msi = timed_graph([&](cudaStream_t cs) {
+        long long nl = 0;
+        for (int k = 0; k < iters; ++k) launch_iteration<M, V>(P, vs, k, cs, nl);
+    });
+    GB_CUDA(cudaGetLastError());
+}
+
+template <class F>
+void by_level(int level, Problem& P, F&& f) {
+    if (level == 0) f(Tag<float, float>{});
+    else if (level == 1) f(Tag<float, double>{});
+    else if (level == 2) f(Tag<double, double>{});
+    else {
+        GB_REQUIRE(!P.has_q, "the BF16 level takes LPs only");
+        ensure_bf16(P);
+        f(Tag<__nv_bfloat16, float>{});
+    }
 }
 
 // Rebuild the row-block schedules of A and A^T for kernel class w (0: FP32 /
@@ -1234,6 +1323,31 @@ int gb_problem_autotune(gb_problem* p, int iters, int* block_nnz, int* max_rows,
             if (block_nnz) block_nnz[w] = P.tune_block_nnz[w][0];
             if (max_rows) max_rows[w] = P.tune_max_rows[w][0];
         }
+    });
+}
+
+int gb_problem_time_kernels_graph(gb_problem* p, int level, int iters, double* ms_primal, double* ms_dual,
+                                  double* ms_iteration) {
+    return guarded([&] {
+        GB_REQUIRE(p && iters > 0 && level >= 0 && level <= 3, "bad arguments");
+        Problem& P = *p->p;
+        GB_REQUIRE(P.solved, "solve once before timing (step sizes come from the solve)");
+        by_level(level, P, [&](auto t) {
+            using T = decltype(t);
+            time_level_graph<typename T::M, typename T::V>(P, iters, ms_primal, ms_dual, ms_iteration);
+        });
+    });
+}
+
+int gb_batch_time_kernels_graph(gb_batch* b, int level, int iters, double* ms_primal, double* ms_dual,
+                                double* ms_iteration) {
+    return guarded([&] {
+        GB_REQUIRE(b && iters > 0 && level >= 0 && level <= 3, "bad arguments");
+        Problem& P = *b->p;
+        by_level(level, P, [&](auto t) {
+            using T = decltype(t);
+            time_level_graph<typename T::M, typename T::V>(P, iters, ms_primal, ms_dual, ms_iteration);
+        });
     });
 }
 

@@ -171,6 +171,13 @@ int gb_problem_time_kernels(gb_problem* p, int level, int iters, double* ms_prim
  * solve, and algorithmic bytes moved by the fused iteration kernels per
  * iteration at each level (index 0..2 = L1..L3). */
 int gb_problem_stats(gb_problem* p, int64_t* launches, double* bytes_per_iter_level);
+/* Same kernels launched back to back: `iters` launches of the fused primal
+ * kernel, then of the fused dual kernel, each captured into a CUDA graph with
+ * programmatic dependent launch exactly as the solve loop issues them and
+ * timed with two CUDA events; also `iters` full iterations.  Mean ms per
+ * launch / per iteration (warm L2). */
+int gb_problem_time_kernels_graph(gb_problem* p, int level, int iters, double* ms_primal, double* ms_dual,
+                                  double* ms_iteration);
 /* Row-split schedule autotuner for one resident problem (see
  * gb_batch_autotune): after a first solve, times candidate (block_nnz,
  * max_rows) cuts of the CSR row blocks -- including cuts into whole waves of
@@ -302,6 +309,8 @@ int gb_batch_autotune(gb_batch* b, int iters, int* block_nnz, int* max_rows, dou
  * 2 = FP64), all instances active, and the algorithmic bytes of one iteration. */
 int gb_batch_time_kernels(gb_batch* b, int level, int iters, double* ms_primal, double* ms_dual, int64_t* launches,
                           double* bytes_per_iter);
+int gb_batch_time_kernels_graph(gb_batch* b, int level, int iters, double* ms_primal, double* ms_dual,
+                                double* ms_iteration);
 void gb_batch_destroy(gb_batch* b);
 
 /* ---------------------------------------------------------------- 3c. problem files

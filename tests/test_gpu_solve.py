@@ -210,3 +210,19 @@ def test_problem_read_from_an_mps_file_solves_like_the_in_memory_one(gb, tmp_pat
     assert a.status == b.status and a.iterations == b.iterations
     np.testing.assert_array_equal(a.x, b.x)
     np.testing.assert_array_equal(a.y, b.y)
+
+
+def test_graph_timed_kernels(gb):
+    lp, _ = load_lp(os.path.join(GOLD, "rand_cfg0.npz"))
+    opt = gb.Options(precision=gb.Precision.Mixed)
+    p = gb.Problem(lp, opt)
+    try:
+        p.solve(opt, fetch=False)
+        for level in (0, 2, 3):
+            t = p.time_kernels_graph(level, 20)
+            assert t["ms_primal"] > 0 and t["ms_dual"] > 0 and t["ms_iteration"] > 0
+            assert t["ms_iteration"] <= 2.0 * (t["ms_primal"] + t["ms_dual"])
+        r = p.solve(opt)  # the timing leaves the problem solvable
+        assert r.status_name == "OPTIMAL"
+    finally:
+        p.close()
