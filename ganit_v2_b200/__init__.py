@@ -8,8 +8,8 @@ Public API (mirrors include/ganit/pdhg.hpp of the reference):
 The compute path is libganit_b200.so (sm_100a); there is no CPU fallback.
 """
 from .lp import LP, Csr
-from .api import (Backend, BatchSolver, DiffSolver, GanitError, Options, Precision, Problem, Result, Status, load_library, set_device,
+from .api import (Backend, BatchSolver, DiffSolver, FactorForm, GanitError, Options, Precision, Problem, Result, Status, load_library, set_device,
                   solve_pdhg_b200, solve_pdhg_gpu, read_mps, LIB_PATH)
 
-__all__ = ["LP", "Csr", "Backend", "BatchSolver", "DiffSolver", "GanitError", "Options", "Precision", "Problem", "Result", "Status",
+__all__ = ["LP", "Csr", "Backend", "BatchSolver", "DiffSolver", "FactorForm", "GanitError", "Options", "Precision", "Problem", "Result", "Status",
            "load_library", "set_device", "solve_pdhg_b200", "solve_pdhg_gpu", "read_mps", "LIB_PATH"]

@@ -163,7 +163,8 @@ EXPORTS = [
     "gb_batch_get_solution", "gb_batch_schedule", "gb_batch_autotune", "gb_batch_time_kernels", "gb_batch_destroy",
     "gb_diff_create", "gb_diff_forward",
     "gb_diff_default_options", "gb_diff_set_options", "gb_diff_backward", "gb_diff_get_info", "gb_diff_tail_start", "gb_diff_destroy",
-    "gb_eval_kkt_noalloc", "gb_read_mps", "gb_model_lp", "gb_model_name", "gb_model_free",
+    "gb_eval_kkt_noalloc", "gb_read_mps", "gb_model_lp", "gb_model_name", "gb_model_free", "gb_factor_detect",
+    "gb_factor_lp", "gb_factor_expand", "gb_factor_free",
 ]
 
 _lib = None
@@ -208,7 +209,8 @@ def load_library(path: str = LIB_PATH):
         "gb_diff_tail_start": (i32, [vp, vp, vp]), "gb_diff_destroy": (None, [vp]),
         "gb_eval_kkt_noalloc": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
         "gb_read_mps": (i32, [C.c_char_p, vp]), "gb_model_lp": (vp, [vp]), "gb_model_name": (C.c_char_p, [vp]),
-        "gb_model_free": (None, [vp]),
+        "gb_model_free": (None, [vp]), "gb_factor_detect": (i32, [vp, vp]), "gb_factor_lp": (vp, [vp]),
+        "gb_factor_expand": (i32, [vp, vp, vp, vp, vp]), "gb_factor_free": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -275,28 +277,68 @@ def read_mps(path: str) -> LP:
     h = C.c_void_p()
     _check(lib.gb_read_mps(os.fsencode(path), C.byref(h)))
     try:
-        v = _GbLp.from_address(lib.gb_model_lp(h))
-        m, n = v.m, v.n
-
-        def arr(ptr, k, dt):
-            if not ptr or k == 0:
-                return np.zeros(k, dtype=dt)
-            ct = C.c_int32 if dt == np.int32 else C.c_double
-            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(k,)).astype(dt, copy=True)
-
-        ptr = arr(v.a_ptr, m + 1, np.int32)
-        nnz = int(ptr[-1]) if m else 0
-        A = Csr(m, n, ptr, arr(v.a_idx, nnz, np.int32), arr(v.a_val, nnz, np.float64))
-        Q = None
-        if v.q_ptr:
-            qp = arr(v.q_ptr, n + 1, np.int32)
-            Q = Csr(n, n, qp, arr(v.q_idx, int(qp[-1]), np.int32), arr(v.q_val, int(qp[-1]), np.float64))
         name = lib.gb_model_name(h).decode(errors="replace") or os.path.basename(path)
-        return LP(A, arr(v.c, n, np.float64), arr(v.l, n, np.float64), arr(v.u, n, np.float64),
-                  arr(v.lo, m, np.float64), arr(v.hi, m, np.float64), obj_const=float(v.obj_const),
-                  maximize=bool(v.maximize), Q=Q, name=name)
+        return _lp_from_view(_GbLp.from_address(lib.gb_model_lp(h)), name=name)
     finally:
         lib.gb_model_free(h)
+
+
+def _lp_from_view(v: "_GbLp", name: str = "") -> LP:
+    """Copy of a library-owned gb_lp (CSR or diagonal-plus-low-rank Hessian)."""
+    m, n = v.m, v.n
+
+    def arr(ptr, k, dt):
+        if not ptr or k == 0:
+            return np.zeros(k, dtype=dt)
+        ct = C.c_int32 if dt == np.int32 else C.c_double
+        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(k,)).astype(dt, copy=True)
+
+    ptr = arr(v.a_ptr, m + 1, np.int32)
+    nnz = int(ptr[-1]) if m else 0
+    A = Csr(m, n, ptr, arr(v.a_idx, nnz, np.int32), arr(v.a_val, nnz, np.float64))
+    Q = F = D = None
+    if v.q_ptr:
+        qp = arr(v.q_ptr, n + 1, np.int32)
+        Q = Csr(n, n, qp, arr(v.q_idx, int(qp[-1]), np.int32), arr(v.q_val, int(qp[-1]), np.float64))
+    if v.q_rank > 0:
+        F = arr(v.q_F, n * v.q_rank, np.float64).reshape(n, v.q_rank)
+        D = arr(v.q_D, n, np.float64)
+    return LP(A, arr(v.c, n, np.float64), arr(v.l, n, np.float64), arr(v.u, n, np.float64),
+              arr(v.lo, m, np.float64), arr(v.hi, m, np.float64), obj_const=float(v.obj_const),
+              maximize=bool(v.maximize), Q=Q, F=F, D=D, name=name)
+
+
+class FactorForm:
+    """A lifted factor-model QP rewritten for the diagonal-plus-low-rank Q x
+    kernel (gb_factor_detect).  ``lp`` is the rewritten problem over x alone;
+    ``expand(x, y)`` maps its solution back to the input's variables and rows.
+    Raises GanitError (GB_ERR_UNSUPPORTED) when the input has no such structure."""
+
+    def __init__(self, lp: LP):
+        self._lib = load_library()
+        self._view = _LpView(lp)
+        self.m_full, self.n_full = lp.m, lp.n
+        h = C.c_void_p()
+        _check(self._lib.gb_factor_detect(C.byref(self._view.s), C.byref(h)))
+        self._h = h
+        self.lp = _lp_from_view(_GbLp.from_address(self._lib.gb_factor_lp(h)), name=(lp.name or "") + "_dplr")
+        self.factors = self.lp.F.shape[1]
+
+    def expand(self, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        xf = np.zeros(self.n_full)
+        yf = np.zeros(self.m_full)
+        _check(self._lib.gb_factor_expand(self._h, _p(x), _p(y), _p(xf), _p(yf)))
+        return xf, yf
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                self._lib.gb_factor_free(self._h)
+                self._h = None
+        except Exception:
+            pass
 
 
 def release_cached_memory() -> None:
@@ -313,16 +355,23 @@ def set_device(device: int) -> None:
     _check(lib.gb_set_device(int(device)))
 
 
-def solve_pdhg_gpu(lp: LP, opt: Options | None = None) -> Result:
+def solve_pdhg_gpu(lp: LP, opt: Options | None = None, out=None) -> Result:
     """Same contract as ganit::solve_pdhg_gpu (include/ganit/pdhg.hpp:44-47):
     scale, restarted PDHG with the precision schedule of ``opt``, FP64
-    certification and unscaling -- all on the B200."""
+    certification and unscaling -- all on the B200.  ``out=(x, y)`` are
+    caller-owned float64 arrays (e.g. page-locked) that receive the solution."""
     lib = load_library()
     v = _LpView(lp)
     o = _opts(opt)
     r = _GbResult()
-    x = np.zeros(lp.n)
-    y = np.zeros(lp.m)
+    if out is None:
+        x = np.zeros(lp.n)
+        y = np.zeros(lp.m)
+    else:
+        x, y = out
+        if not (x.dtype == np.float64 and y.dtype == np.float64 and x.shape == (lp.n,) and y.shape == (lp.m,)
+                and x.flags.c_contiguous and y.flags.c_contiguous):
+            raise ValueError("out must be two contiguous float64 arrays of n and m entries")
     _check(lib.gb_solve(C.addressof(v.s), C.addressof(o), C.addressof(r), _p(x), _p(y)))
     return _result(r, x, y)
 

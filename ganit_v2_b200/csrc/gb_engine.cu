@@ -21,15 +21,31 @@ namespace gb {
 thread_local std::string g_last_error;
 thread_local int g_device = 0;
 
+// Compute capability and SM count of a device, looked up once per device
+// (cudaDeviceGetAttribute; a full cudaGetDeviceProperties costs milliseconds).
 inline void check_device(int dev, int* sms) {
+    static std::mutex mu;
+    static std::vector<std::array<int, 3>> seen;  // device, major*10+minor, SMs
+    {
+        std::lock_guard<std::mutex> g(mu);
+        for (const auto& d : seen)
+            if (d[0] == dev) {
+                *sms = d[2];
+                return;
+            }
+    }
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) throw Error(GB_ERR_NODEVICE, "no CUDA device");
     GB_REQUIRE(dev >= 0 && dev < count, "device index out of range");
-    cudaDeviceProp prop;
-    GB_CUDA(cudaGetDeviceProperties(&prop, dev));
-    if (prop.major < 10) throw Error(GB_ERR_NODEVICE, "libganit_b200 is built for sm_100a (B200); found sm_" +
-                                                          std::to_string(prop.major) + std::to_string(prop.minor));
-    *sms = prop.multiProcessorCount;
+    int major = 0, minor = 0, nsm = 0;
+    GB_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    GB_CUDA(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev));
+    GB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    if (major < 10) throw Error(GB_ERR_NODEVICE, "libganit_b200 is built for sm_100a (B200); found sm_" +
+                                                     std::to_string(major) + std::to_string(minor));
+    std::lock_guard<std::mutex> g(mu);
+    seen.push_back({dev, major * 10 + minor, nsm});
+    *sms = nsm;
 }
 
 // Opt a kernel into the dynamic shared memory it needs.
@@ -47,7 +63,12 @@ void validate_lp(const gb_lp* lp) {
     for (int i = 0; i < lp->m; ++i) GB_REQUIRE(lp->a_ptr[i + 1] >= lp->a_ptr[i], "A.ptr must be nondecreasing");
     const long long nnz = lp->a_ptr[lp->m];
     GB_REQUIRE(nnz == 0 || (lp->a_idx && lp->a_val), "missing A.idx/val");
-    for (long long p = 0; p < nnz; ++p) GB_REQUIRE(lp->a_idx[p] >= 0 && lp->a_idx[p] < lp->n, "A.idx out of range");
+    int lo_idx = 0, hi_idx = 0;  // one vectorisable min / max pass instead of a branch per entry
+    for (long long p = 0; p < nnz; ++p) {
+        lo_idx = std::min(lo_idx, lp->a_idx[p]);
+        hi_idx = std::max(hi_idx, lp->a_idx[p]);
+    }
+    GB_REQUIRE(lo_idx >= 0 && (nnz == 0 || hi_idx < lp->n), "A.idx out of range");
     for (int j = 0; j < lp->n; ++j) GB_REQUIRE(!(lp->l[j] > lp->u[j]), "column bound l > u");
     if (lp->q_rank > 0) {
         GB_REQUIRE(lp->q_F && lp->q_D, "DPLR Hessian needs q_F and q_D");
@@ -217,6 +238,7 @@ __global__ void k_fill_segments(const int* off, int* out) {
 // of `count` instances.
 Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     GB_REQUIRE(count >= 1 && lps != nullptr, "need at least one problem");
+    const auto t0 = std::chrono::steady_clock::now();  // setup_seconds covers validation too
     for (int k = 0; k < count; ++k) validate_lp(&lps[k]);
     if (count > 1)
         for (int k = 0; k < count; ++k)
@@ -228,7 +250,6 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     init_kernel_attrs();
     GB_CUDA(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
     cudaStream_t s = P->stream;
-    const auto t0 = std::chrono::steady_clock::now();
     P->count = count;
     P->row_off.assign(count + 1, 0);
     P->col_off.assign(count + 1, 0);

@@ -325,6 +325,23 @@ const gb_lp* gb_model_lp(const gb_model* model);
 const char* gb_model_name(const gb_model* model);
 void gb_model_free(gb_model* model);
 
+/* Factor-model rewrite (no reference counterpart).  A QP with a diagonal CSR
+ * Hessian in the lifted form of a factor risk model -- free columns f_k with
+ * curvature q_k > 0, each in exactly one equality row a_k f_k + g'x = b_k
+ * that holds no other such column (the form bench/gen_portfolio.py of the
+ * reference writes) -- is rewritten over x alone with Q = 2 (F F^T + diag(D)),
+ * F[:, k] = sqrt(q_k / 2) (-row_k / a_k), D = diag(Q_xx) / 2, for the engine's
+ * diagonal-plus-low-rank kernel.  GB_ERR_UNSUPPORTED when no such structure
+ * (or more than 128 factors, or a non-diagonal / indefinite Hessian, or a
+ * maximisation).  gb_factor_expand maps a solution (x, y) of the rewritten
+ * problem back: x_full (n of the input), y_full (m of the input), with
+ * f_k = (b_k - g'x) / a_k and y_k = (c_k + q_k f_k) / a_k. */
+typedef struct gb_factor gb_factor;
+int gb_factor_detect(const gb_lp* qp, gb_factor** out);
+const gb_lp* gb_factor_lp(const gb_factor* f);
+int gb_factor_expand(const gb_factor* f, const double* x, const double* y, double* x_full, double* y_full);
+void gb_factor_free(gb_factor* f);
+
 /* ---------------------------------------------------------------- 3b. differentiable solving
  * No counterpart in the reference (it differentiates run_pdhg,
  * src/pdhg_impl.hpp:243-328).  LPs only.

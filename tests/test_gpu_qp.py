@@ -38,3 +38,20 @@ def test_dplr_portfolio_matches_lifted_oracle(qp, oracle_built, prec, tol):
     x = r.x
     obj = x @ (F @ (F.T @ x)) + x @ (D * x) + dplr.c @ x
     assert abs(obj - r.pobj) <= 1e-6 * (1 + abs(obj))
+
+
+def test_factor_rewrite_solves_the_lifted_file_form():
+    """A lifted factor model solved through the rewrite (DPLR kernel) and the
+    expanded solution agree with solving the lifted form itself (CSR Hessian)."""
+    import ganit_v2_b200 as gb
+
+    lifted = W.portfolio_qp(2000, 10, seed=13, lifted=True)
+    opt = gb.Options(tol=1e-6, precision=gb.Precision.Double)
+    ff = gb.FactorForm(lifted)
+    r = gb.solve_pdhg_gpu(ff.lp, opt)
+    s = gb.solve_pdhg_gpu(lifted, opt)
+    assert r.status_name == s.status_name == "OPTIMAL"
+    assert abs(r.pobj - s.pobj) <= 10 * 1e-6 * (1 + abs(s.pobj))
+    xf, yf = ff.expand(r.x, r.y)
+    assert np.linalg.norm(xf - s.x) <= 1e-3 * (1 + np.linalg.norm(s.x))
+    assert np.linalg.norm(yf - s.y) <= 1e-2 * (1 + np.linalg.norm(s.y))
