@@ -124,6 +124,17 @@ class _GbResult(C.Structure):
                 ("bf16_iterations", C.c_int64)]
 
 
+class _GbBranchCand(C.Structure):
+    _fields_ = [("z", C.c_double * 2), ("cert", C.c_double * 2), ("status", C.c_int32 * 2),
+                ("iterations", C.c_int64 * 2), ("score", C.c_double)]
+
+
+class _GbBranchDecision(C.Structure):
+    _fields_ = [("action", C.c_int32), ("var", C.c_int32), ("lo", C.c_double), ("hi", C.c_double),
+                ("est", C.c_double * 2), ("cert", C.c_double * 2), ("children_solved", C.c_int32),
+                ("seconds", C.c_double)]
+
+
 class _GbScaledLp(C.Structure):
     _fields_ = [("m", C.c_int32), ("n", C.c_int32)] + [
         (k, C.c_void_p) for k in ("a_ptr", "a_idx", "a_val", "at_ptr", "at_idx", "at_val", "q_ptr", "q_idx", "q_val",
@@ -164,7 +175,7 @@ EXPORTS = [
     "gb_diff_create", "gb_diff_forward",
     "gb_diff_default_options", "gb_diff_set_options", "gb_diff_backward", "gb_diff_get_info", "gb_diff_tail_start", "gb_diff_destroy",
     "gb_eval_kkt_noalloc", "gb_read_mps", "gb_model_lp", "gb_model_name", "gb_model_free", "gb_factor_detect",
-    "gb_factor_lp", "gb_factor_expand", "gb_factor_free",
+    "gb_factor_lp", "gb_factor_expand", "gb_factor_free", "gb_model_is_int", "gb_strong_branch",
 ]
 
 _lib = None
@@ -211,6 +222,8 @@ def load_library(path: str = LIB_PATH):
         "gb_read_mps": (i32, [C.c_char_p, vp]), "gb_model_lp": (vp, [vp]), "gb_model_name": (C.c_char_p, [vp]),
         "gb_model_free": (None, [vp]), "gb_factor_detect": (i32, [vp, vp]), "gb_factor_lp": (vp, [vp]),
         "gb_factor_expand": (i32, [vp, vp, vp, vp, vp]), "gb_factor_free": (None, [vp]),
+        "gb_model_is_int": (vp, [vp]),
+        "gb_strong_branch": (i32, [vp, vp, i32, vp, dbl, dbl, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -278,7 +291,12 @@ def read_mps(path: str) -> LP:
     _check(lib.gb_read_mps(os.fsencode(path), C.byref(h)))
     try:
         name = lib.gb_model_name(h).decode(errors="replace") or os.path.basename(path)
-        return _lp_from_view(_GbLp.from_address(lib.gb_model_lp(h)), name=name)
+        lp = _lp_from_view(_GbLp.from_address(lib.gb_model_lp(h)), name=name)
+        if lp.n:
+            flags = np.ctypeslib.as_array(C.cast(lib.gb_model_is_int(h), C.POINTER(C.c_uint8)), shape=(lp.n,))
+            if flags.any():
+                lp.is_int = flags.astype(bool)
+        return lp
     finally:
         lib.gb_model_free(h)
 
@@ -339,6 +357,78 @@ class FactorForm:
                 self._h = None
         except Exception:
             pass
+
+
+BRANCH_VAR, BRANCH_TIGHTEN, BRANCH_NODE_INFEASIBLE = 0, -1, -2
+
+
+@dataclass
+class StrongBranch:
+    """Outcome of gb_strong_branch: per candidate (rows) and child (columns:
+    down, up) the objective estimate, certified bound, status and iterations;
+    the candidates' scores; and the decision Mip::select_branch would take
+    (action BRANCH_VAR / BRANCH_TIGHTEN / BRANCH_NODE_INFEASIBLE)."""
+
+    candidates: np.ndarray
+    z: np.ndarray
+    cert: np.ndarray
+    status: np.ndarray
+    iterations: np.ndarray
+    score: np.ndarray
+    action: int
+    var: int
+    lo: float
+    hi: float
+    est: np.ndarray
+    cert_choice: np.ndarray
+    children_solved: int
+    seconds: float
+
+
+def fractional(x, is_int, int_tol: float = 1e-6) -> np.ndarray:
+    """Integer columns whose value is fractional beyond int_tol (Mip::fractional,
+    src/mip.cpp:256-263), in column order."""
+    x = np.asarray(x, dtype=np.float64)
+    f = x - np.floor(x)
+    return np.flatnonzero(np.asarray(is_int, dtype=bool) & (f > int_tol) & (f < 1.0 - int_tol)).astype(np.int32)
+
+
+def most_fractional(x, cols, k: int) -> np.ndarray:
+    """The k columns of `cols` closest to half-integral, most fractional first
+    (the expert order of full strong branching, src/mip.cpp:709-714; stable)."""
+    x = np.asarray(x, dtype=np.float64)
+    cols = np.asarray(cols, dtype=np.int32)
+    f = x[cols] - np.floor(x[cols])
+    order = np.argsort(-np.minimum(f, 1.0 - f), kind="stable")
+    return cols[order[:k]]
+
+
+def strong_branch(lp: LP, x, candidates, node_obj: float, cutoff: float = float("inf"),
+                  opt: Options | None = None) -> StrongBranch:
+    """Strong-branch the candidate columns of a MILP node LP on the GPU
+    (gb_strong_branch): both children of every candidate solved as one batch,
+    each with a rigorous bound from its duals.  Objectives in minimisation form."""
+    lib = load_library()
+    view = _LpView(lp)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    cand = np.ascontiguousarray(candidates, dtype=np.int32)
+    if x.shape != (lp.n,) or cand.ndim != 1 or cand.size == 0:
+        raise ValueError("x must have n entries and candidates at least one")
+    o = _opts(opt)
+    out = (_GbBranchCand * cand.size)()
+    dec = _GbBranchDecision()
+    _check(lib.gb_strong_branch(C.byref(view.s), _p(x), int(cand.size), _p(cand), float(node_obj), float(cutoff),
+                                C.addressof(o), out, C.byref(dec)))
+    return StrongBranch(
+        candidates=cand.copy(),
+        z=np.array([[c.z[0], c.z[1]] for c in out]),
+        cert=np.array([[c.cert[0], c.cert[1]] for c in out]),
+        status=np.array([[c.status[0], c.status[1]] for c in out], dtype=np.int32),
+        iterations=np.array([[c.iterations[0], c.iterations[1]] for c in out], dtype=np.int64),
+        score=np.array([c.score for c in out]),
+        action=int(dec.action), var=int(dec.var), lo=float(dec.lo), hi=float(dec.hi),
+        est=np.array(list(dec.est)), cert_choice=np.array(list(dec.cert)),
+        children_solved=int(dec.children_solved), seconds=float(dec.seconds))
 
 
 def release_cached_memory() -> None:

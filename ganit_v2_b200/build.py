@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libganit_b200.so")
-SOURCES = ["gb_engine.cu", "gb_backend.cu", "gb_diff.cu", "gb_noalloc.cu", "gb_pool.cu", "gb_mps.cpp", "gb_factor.cpp"]
+SOURCES = ["gb_engine.cu", "gb_backend.cu", "gb_diff.cu", "gb_noalloc.cu", "gb_pool.cu", "gb_branch.cu", "gb_mps.cpp", "gb_factor.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]

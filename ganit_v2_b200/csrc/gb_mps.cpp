@@ -2,7 +2,8 @@
 //
 // Same format rules as the reference reader (src/mps.cpp:69-272): free-form
 // whitespace-separated fields; sections NAME, OBJSENSE (header argument or
-// next line), ROWS, COLUMNS (with 'MARKER' INTORG/INTEND lines skipped),
+// next line), ROWS, COLUMNS ('MARKER' INTORG/INTEND lines mark the columns
+// between them integer; bound types UI, LI and BV do too),
 // RHS, RANGES, BOUNDS, QUADOBJ (lower triangle, mirrored), QMATRIX/QSECTION
 // (full), ENDATA; the first N row is the objective, further N rows are
 // ignored; an objective RHS entry v gives obj_const = -v; RHS / RANGES lines
@@ -98,6 +99,7 @@ class Parser {
     double obj_const = 0.0;
     std::vector<int32_t> a_ptr, a_idx, q_ptr, q_idx;
     std::vector<double> a_val, q_val, c, l, u, lo, hi;
+    std::vector<unsigned char> is_int;
 
    private:
     enum Section { kNone, kName, kSense, kRows, kCols, kRhs, kRanges, kBounds, kQuadObj, kQMatrix };
@@ -177,7 +179,11 @@ class Parser {
     }
 
     void column_line() {
-        if (tok_.size() >= 3 && tok_[1] == "'MARKER'") return;  // integrality markers: LP relaxation
+        if (tok_.size() >= 3 && tok_[1] == "'MARKER'") {
+            if (tok_[2] == "'INTORG'") int_mode_ = true;
+            else if (tok_[2] == "'INTEND'") int_mode_ = false;
+            return;
+        }
         if (tok_[0] != cur_name_) {
             cur_name_ = tok_[0];
             cur_ = n++;
@@ -185,6 +191,7 @@ class Parser {
             c.push_back(0.0);
             l.push_back(0.0);
             u.push_back(kInf);
+            is_int.push_back(int_mode_ ? 1 : 0);
             lower_given_.push_back(0);
         }
         for (size_t k = 1; k + 1 < tok_.size(); k += 2) {
@@ -241,9 +248,11 @@ class Parser {
         if (t == "UP" || t == "UI") {
             u[j] = v;
             if (v < 0 && l[j] == 0.0 && !lower_given_[j]) l[j] = -kInf;
+            if (t == "UI") is_int[j] = 1;
         } else if (t == "LO" || t == "LI") {
             l[j] = v;
             lower_given_[j] = 1;
+            if (t == "LI") is_int[j] = 1;
         } else if (t == "FX") {
             l[j] = u[j] = v;
             lower_given_[j] = 1;
@@ -260,6 +269,7 @@ class Parser {
             l[j] = 0.0;
             u[j] = 1.0;
             lower_given_[j] = 1;
+            is_int[j] = 1;
         } else {
             fail("unknown bound type '" + t + "'");
         }
@@ -299,6 +309,7 @@ class Parser {
     std::vector<std::string> tok_;
     std::string obj_, cur_name_;
     int cur_ = -1;
+    bool int_mode_ = false;
     std::unordered_map<std::string, int> rows_, cols_;
     std::unordered_set<std::string> extra_n_;
     std::vector<char> row_type_, lower_given_;
@@ -357,6 +368,8 @@ int gb_read_mps(const char* path, gb_model** out) {
 const gb_lp* gb_model_lp(const gb_model* mdl) { return mdl ? &mdl->view : nullptr; }
 
 const char* gb_model_name(const gb_model* mdl) { return mdl ? mdl->p.name.c_str() : nullptr; }
+
+const unsigned char* gb_model_is_int(const gb_model* mdl) { return mdl ? mdl->p.is_int.data() : nullptr; }
 
 void gb_model_free(gb_model* mdl) { delete mdl; }
 

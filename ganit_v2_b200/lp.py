@@ -80,6 +80,7 @@ class LP:
     D: Optional[np.ndarray] = None   # n diagonal of the same
     name: str = "lp"
     meta: dict = field(default_factory=dict)
+    is_int: Optional[np.ndarray] = None  # n bools: integer columns of a MILP (the LP solvers ignore them)
 
     def __post_init__(self):
         for k in ("c", "l", "u", "lo", "hi"):

@@ -367,3 +367,50 @@ def infeasible_lp(m: int = 200, n: int = 500, seed: int = 3) -> LP:
     lo = np.concatenate([base.lo, [-np.inf, bval]])
     hi = np.concatenate([base.hi, [bval - 1.0, np.inf]])
     return LP(Csr.from_scipy(A), base.c, base.l, base.u, lo, hi, name=f"infeas_m{m}_n{n}_s{seed}")
+
+
+def milp_node(n: int = 120, knapsacks: int = 8, density: float = 0.3, up_blocked: int = 2, down_blocked: int = 2,
+              both_blocked: int = 0, seed: int = 11) -> LP:
+    """Root node of a synthetic MILP for strong branching: a multi-dimensional
+    knapsack (maximise profit, written as minimise -profit; integer columns in
+    [0, U_j], U_j in {1, 2, 3}; rows W x <= 0.3 * W U) whose LP relaxation has
+    fractional columns, plus three planted kinds of integer column:
+
+    * ``up_blocked``: a row 5 x_j <= 3 (so x_j <= 0.6) and a high profit --
+      the relaxation takes x_j = 0.6 and the up child (x_j >= 1) is infeasible;
+    * ``down_blocked``: a row x_j >= 0.4 and a negative profit -- the relaxation
+      takes x_j = 0.4 and the down child (x_j <= 0) is infeasible;
+    * ``both_blocked``: both rows -- either child is infeasible.
+
+    ``is_int`` marks every column; ``meta`` lists the planted columns."""
+    rng = np.random.default_rng(seed)
+    nk = n + up_blocked + down_blocked + both_blocked
+    U = rng.integers(1, 4, size=nk).astype(np.float64)
+    p = rng.uniform(1.0, 10.0, size=nk)
+    W = sp.random(knapsacks, n, density=density, random_state=np.random.RandomState(seed),
+                  data_rvs=lambda k: np.random.RandomState(seed + 1).uniform(1.0, 10.0, size=k)).tocsr()
+    W = sp.hstack([W, sp.csr_matrix((knapsacks, nk - n))], format="csr")
+    cap = 0.3 * (W @ U)
+    up = np.arange(n, n + up_blocked)
+    down = np.arange(n + up_blocked, n + up_blocked + down_blocked)
+    both = np.arange(n + up_blocked + down_blocked, nk)
+    U[up] = U[down] = U[both] = 1.0
+    p[up] = 50.0
+    p[down] = -1.0
+    p[both] = 1.0
+    rows = [W]
+    lo = [np.full(knapsacks, -np.inf)]
+    hi = [cap]
+    for j in np.concatenate([up, both]):
+        rows.append(sp.csr_matrix(([5.0], ([0], [j])), shape=(1, nk)))
+        lo.append([-np.inf])
+        hi.append([3.0])
+    for j in np.concatenate([down, both]):
+        rows.append(sp.csr_matrix(([1.0], ([0], [j])), shape=(1, nk)))
+        lo.append([0.4])
+        hi.append([np.inf])
+    A = sp.vstack(rows, format="csr")
+    A.sort_indices()
+    return LP(Csr.from_scipy(A), -p, np.zeros(nk), U, np.concatenate(lo), np.concatenate(hi),
+              name=f"milp_node_n{n}_k{knapsacks}_s{seed}", is_int=np.ones(nk, dtype=bool),
+              meta={"up_blocked": up, "down_blocked": down, "both_blocked": both})

@@ -316,13 +316,17 @@ void gb_batch_destroy(gb_batch* b);
 /* ---------------------------------------------------------------- 3c. problem files
  * Replaces ganit::read_mps (src/mps.cpp:69-272) for callers that feed the
  * engine directly from an MPS / QPS file, with the same format rules
- * (sections, N rows, RHS / RANGES / BOUNDS semantics, QUADOBJ mirrored,
- * integrality markers ignored).  gb_model_lp returns a view of the model,
- * valid until gb_model_free, that gb_solve / gb_problem_create accept. */
+ * (sections, N rows, RHS / RANGES / BOUNDS semantics, QUADOBJ mirrored).
+ * gb_model_lp returns a view of the model, valid until gb_model_free, that
+ * gb_solve / gb_problem_create accept; gb_model_is_int its integrality (n
+ * bytes, 1 = integer: columns between 'MARKER' INTORG / INTEND lines and
+ * columns with a UI, LI or BV bound, as src/mps.cpp:149-229), which the LP
+ * solvers ignore (they solve the relaxation). */
 typedef struct gb_model gb_model;
 int gb_read_mps(const char* path, gb_model** out);
 const gb_lp* gb_model_lp(const gb_model* model);
 const char* gb_model_name(const gb_model* model);
+const unsigned char* gb_model_is_int(const gb_model* model);
 void gb_model_free(gb_model* model);
 
 /* Factor-model rewrite (no reference counterpart).  A QP with a diagonal CSR
@@ -341,6 +345,45 @@ int gb_factor_detect(const gb_lp* qp, gb_factor** out);
 const gb_lp* gb_factor_lp(const gb_factor* f);
 int gb_factor_expand(const gb_factor* f, const double* x, const double* y, double* x_full, double* y_full);
 void gb_factor_free(gb_factor* f);
+
+/* ---------------------------------------------------------------- 3d. strong branching
+ * Replaces the per-candidate strong-branching loop of Mip::select_branch
+ * (src/mip.cpp:727-783), where each child LP is a warm dual-simplex re-solve
+ * followed by Mip::safe_bound (src/mip.cpp:356-410).  Here the 2 * count
+ * children of the candidate columns cand[] of the node LP `lp` (its column
+ * bounds are the node's) -- down: u_j = floor(x_j), up: l_j = ceil(x_j) --
+ * are solved together as one gb_batch with `opt`, and each child's rigorous
+ * Lagrangian lower bound is formed on the device from its duals with
+ * directed rounding.  Every x[cand[k]] must be fractional; LPs only.
+ * Objectives are in minimisation form (a maximisation LP's are negated), and
+ * node_obj / cutoff are too (cutoff = INFINITY: no incumbent).
+ * Per child (index 0 = down, 1 = up), as src/mip.cpp:750-763: z = +INF when
+ * the child is primal infeasible (also when its bounds cross) or its
+ * certified bound is >= cutoff; else its objective when GB_OPTIMAL; else
+ * max(node_obj, cert), or node_obj when cert = -INF (not certifiable). */
+typedef struct {
+    double z[2];          /* child objective estimate */
+    double cert[2];       /* certified lower bound (+INF: infeasible; -INF: none) */
+    int32_t status[2];    /* GB_OPTIMAL ... of the child solve */
+    int64_t iterations[2];
+    double score;         /* max(z0 - node_obj, 1e-6) * max(z1 - node_obj, 1e-6); 0 if a z is +INF */
+} gb_branch_cand;
+/* The decision select_branch takes, scanning cand[] in order: the first
+ * candidate with both children +INF makes the node infeasible, the first
+ * with one makes the column tightened to the other side; else the largest
+ * score wins (first on ties). */
+enum { GB_BRANCH_VAR = 0, GB_BRANCH_TIGHTEN = -1, GB_BRANCH_NODE_INFEASIBLE = -2 };
+typedef struct {
+    int32_t action;       /* GB_BRANCH_* (the return value of select_branch) */
+    int32_t var;          /* column branched on / tightened / found infeasible */
+    double lo, hi;        /* GB_BRANCH_TIGHTEN: the column's new bounds */
+    double est[2];        /* GB_BRANCH_VAR: est_down / est_up of the chosen column */
+    double cert[2];       /* GB_BRANCH_VAR: cert_down / cert_up of the chosen column */
+    int32_t children_solved; /* children in the batch (bounds that cross need no solve) */
+    double seconds;       /* wall time of the call */
+} gb_branch_decision;
+int gb_strong_branch(const gb_lp* lp, const double* x, int32_t count, const int32_t* cand, double node_obj,
+                     double cutoff, const gb_options* opt, gb_branch_cand* out, gb_branch_decision* decision);
 
 /* ---------------------------------------------------------------- 3b. differentiable solving
  * No counterpart in the reference (it differentiates run_pdhg,

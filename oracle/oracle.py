@@ -262,12 +262,15 @@ def ref_read_mps(path: str):
         lib.ref_mps_copy.argtypes = [C.c_void_p] * 13
         lib.ref_mps_copy(h, _p(ptr), _p(idx), _p(val), _p(c), _p(l), _p(u), _p(lo), _p(hi), _p(oc), _p(qptr),
                          _p(qidx), _p(qval))
+        is_int = np.zeros(n, np.uint8)
+        lib.ref_mps_is_int.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ref_mps_is_int(h, _p(is_int))
     finally:
         lib.ref_mps_free.argtypes = [C.c_void_p]
         lib.ref_mps_free(h)
     Q = Csr(n, n, qptr, qidx, qval) if qnnz else None
     return LP(Csr(m, n, ptr, idx, val), c, l, u, lo, hi, obj_const=float(oc[0]), maximize=bool(maxi), Q=Q,
-              name=os.path.basename(path))
+              name=os.path.basename(path), is_int=is_int.astype(bool) if is_int.any() else None)
 
 
 def ref_dual_simplex(lp, time_limit: float = 300.0) -> dict:
@@ -289,3 +292,109 @@ def ref_dual_simplex(lp, time_limit: float = 300.0) -> dict:
            _p(head), _p(status), C.addressof(iters))
     return {"status": int(rc), "objective": obj.value, "x": x, "y": y, "head": head, "var_status": status,
             "iterations": iters.value}
+
+
+# ---- strong branching (src/mip.cpp:668-783) with the reference dual simplex
+SIMPLEX_OPTIMAL, SIMPLEX_INFEASIBLE = 0, 1
+
+
+def _child(lp, j: int, lo: float, hi: float):
+    from dataclasses import replace
+
+    l = lp.l.copy()
+    u = lp.u.copy()
+    l[j], u[j] = lo, hi
+    return replace(lp, l=l, u=u, meta={})
+
+
+def _min_form(lp):
+    from dataclasses import replace
+
+    if not lp.maximize:
+        return lp
+    return replace(lp, c=-lp.c, obj_const=-lp.obj_const, maximize=False, meta={})
+
+
+def strong_branch_reference(lp, x, candidates, node_obj: float, cutoff: float = np.inf) -> dict:
+    """The strong-branching loop of Mip::select_branch (src/mip.cpp:727-783)
+    with every child solved to optimality by the reference dual simplex (cold,
+    no iteration limit): z per child (+inf when infeasible or >= cutoff), the
+    scores, and the decision (action 0 branch / -1 tighten / -2 infeasible,
+    column, new bounds).  Minimisation form throughout."""
+    lpm = _min_form(lp)
+    eps = 1e-6
+    k = len(candidates)
+    z = np.full((k, 2), np.nan)
+    status = np.zeros((k, 2), np.int32)
+    for t, j in enumerate(candidates):
+        v = float(x[j])
+        for d, (lo, hi) in enumerate(((lpm.l[j], np.floor(v)), (np.ceil(v), lpm.u[j]))):
+            if not lo <= hi:
+                status[t, d] = SIMPLEX_INFEASIBLE
+                z[t, d] = np.inf
+                continue
+            r = ref_dual_simplex(_child(lpm, int(j), lo, hi))
+            status[t, d] = r["status"]
+            if r["status"] == SIMPLEX_INFEASIBLE:
+                z[t, d] = np.inf
+            elif r["status"] == SIMPLEX_OPTIMAL:
+                z[t, d] = np.inf if r["objective"] >= cutoff else r["objective"]
+            else:
+                raise RuntimeError(f"dual simplex status {r['status']} on a child")
+    score = np.zeros(k)
+    action, var, blo, bhi, best = 0, int(candidates[0]), np.nan, np.nan, -1.0
+    for t, j in enumerate(candidates):
+        inf0, inf1 = not np.isfinite(z[t, 0]), not np.isfinite(z[t, 1])
+        if inf0 and inf1:
+            action, var = -2, int(j)
+            break
+        if inf0 or inf1:
+            v = float(x[j])
+            action, var = -1, int(j)
+            blo, bhi = (np.ceil(v), lpm.u[j]) if inf0 else (lpm.l[j], np.floor(v))
+            break
+        score[t] = max(z[t, 0] - node_obj, eps) * max(z[t, 1] - node_obj, eps)
+        if score[t] > best:
+            best, var = score[t], int(j)
+    return {"z": z, "status": status, "score": score, "action": action, "var": var, "lo": blo, "hi": bhi}
+
+
+def lagrangian_bound_exact(lp, y, j: int, lo: float, hi: float) -> float:
+    """EXACT value (rational arithmetic) of the Lagrangian bound the reference
+    certifies child bounds with (Mip::safe_bound, src/mip.cpp:356-410), for
+    duals y of the child with column j's bounds set to [lo, hi]:
+        sum_i min(y_i lo_i, y_i hi_i) + sum_j min_{x_j in [l_j, u_j]} (c - A'y)_j x_j,
+    y_i clamped to <= 0 on rows without a finite lower side and >= 0 without
+    a finite upper side; -inf when a column with an infinite bound has a
+    reduced cost of the wrong sign.  Minimisation form."""
+    from fractions import Fraction as F
+
+    lpm = _min_form(lp)
+    m, n = lpm.m, lpm.n
+    yy = []
+    total = F(0)
+    for i in range(m):
+        yi = float(y[i])
+        if not np.isfinite(lpm.lo[i]):
+            yi = min(yi, 0.0)
+        if not np.isfinite(lpm.hi[i]):
+            yi = max(yi, 0.0)
+        yy.append(F(yi))
+        if yi > 0:
+            total += F(yi) * F(float(lpm.lo[i]))
+        elif yi < 0:
+            total += F(yi) * F(float(lpm.hi[i]))
+    d = [F(float(v)) for v in lpm.c]
+    ptr, idx, val = lpm.A.ptr, lpm.A.idx, lpm.A.val
+    for i in range(m):
+        if yy[i] == 0:
+            continue
+        for t in range(ptr[i], ptr[i + 1]):
+            d[idx[t]] -= yy[i] * F(float(val[t]))
+    for c in range(n):
+        l, u = (lo, hi) if c == j else (float(lpm.l[c]), float(lpm.u[c]))
+        if (not np.isfinite(l) and d[c] > 0) or (not np.isfinite(u) and d[c] < 0):
+            return -np.inf
+        cands = [d[c] * F(v) for v in (l, u) if np.isfinite(v)]
+        total += min(cands) if cands else F(0)
+    return total  # a Fraction: compare it with floats exactly

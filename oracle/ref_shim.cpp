@@ -155,6 +155,12 @@ void ref_mps_copy(void* hp, int* ptr, int* idx, double* val, double* c, double* 
     }
 }
 
+// is_int (n bytes) of the reference reader's LP
+void ref_mps_is_int(void* hp, unsigned char* out) {
+    const LP& lp = static_cast<ref_mps*>(hp)->lp;
+    for (int j = 0; j < lp.n; ++j) out[j] = j < (int)lp.is_int.size() && lp.is_int[j] ? 1 : 0;
+}
+
 void ref_mps_free(void* hp) { delete static_cast<ref_mps*>(hp); }
 
 // ---- dual simplex (src/simplex.hpp:37-93): exact vertex, basis and duals.

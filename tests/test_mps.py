@@ -41,6 +41,9 @@ def test_matches_the_reference_reader(gb, oracle_built, path):
     np.testing.assert_allclose(a.A.val, b.A.val, rtol=1e-15, atol=0)  # duplicates may sum in another order
     for k in ("c", "l", "u", "lo", "hi"):
         np.testing.assert_array_equal(getattr(a, k), getattr(b, k), err_msg=k)
+    assert (a.is_int is None) == (b.is_int is None)
+    if a.is_int is not None:
+        np.testing.assert_array_equal(a.is_int, b.is_int)
     assert (a.Q is None) == (b.Q is None)
     if a.Q is not None:
         np.testing.assert_array_equal(a.Q.ptr, b.Q.ptr)
@@ -125,6 +128,8 @@ def test_every_section_and_rule(gb, tmp_path):
     expect = np.zeros((9, 9))
     expect[0, 0], expect[0, 1], expect[1, 0] = 2.0, 0.5, 0.5  # QUADOBJ lower triangle mirrored
     np.testing.assert_array_equal(Q, expect)
+    # integer: X2 between the markers, X8 (BV), X9 (LI / UI)
+    np.testing.assert_array_equal(lp.is_int, [0, 1, 0, 0, 0, 0, 0, 1, 1])
 
 
 @pytest.mark.parametrize("text,msg", [
