@@ -265,6 +265,60 @@ def qp_measure(steps: int = 2) -> dict:
     return out
 
 
+def branch_measure(cpu: bool, steps: int = 3, candidates: int = 32) -> dict:
+    """Strong branching of a synthetic MILP node (workloads.milp_node: 5000
+    integer columns, 200 knapsack rows at 2% density, seed 11): the node LP
+    solved on the GPU (FP64, 1e-7), its `candidates` most fractional columns
+    strong-branched -- 2 * candidates child LPs as one batch, mixed precision to
+    1e-6 from the node's point, rigorous child bounds -- through
+    gb_strong_branch (host arrays in and out, wall clock).  CPU leg: the
+    reference's own loop (warm dual simplex per child, its default limit of 60
+    iterations, src/mip.cpp:738-760) from the same node point and candidates,
+    the node's simplex solve before it untimed."""
+    import numpy as np
+
+    import ganit_v2_b200 as gb
+    from ganit_v2_b200 import workloads as W
+
+    lp = W.milp_node(n=5000, knapsacks=200, density=0.02, up_blocked=0, down_blocked=0, seed=11)
+    root = gb.solve_pdhg_gpu(lp, gb.Options(tol=1e-7, precision=gb.Precision.Double))
+    x, y, z = root.x, root.y, root.pobj
+    cands = gb.most_fractional(x, gb.fractional(x, lp.is_int), candidates)
+    opt = gb.Options(tol=1e-6, precision=gb.Precision.Mixed)
+    sb = gb.strong_branch(lp, x, cands, z, opt=opt, y=y)
+    secs = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        sb = gb.strong_branch(lp, x, cands, z, opt=opt, y=y)
+        secs.append(time.perf_counter() - t0)
+    t = min(secs)
+    out = {"workload": "MILP node: multi-dimensional knapsack, 5000 integer columns, 200 rows, 2% density "
+                       f"(nnz {lp.A.nnz}); {len(cands)} most fractional candidates, {2 * len(cands)} child LPs",
+           "children_per_s": 2 * len(cands) / t, "seconds": t, "seconds_all": secs,
+           "children_solved": sb.children_solved, "action": sb.action, "var": sb.var,
+           "iterations_mean": float(sb.iterations.mean()), "iterations_max": int(sb.iterations.max()),
+           "settings": "children: mixed precision to 1e-6 relative KKT, started from the node point; every "
+                       "child bound certified on the device (directed rounding)"}
+    if cpu:
+        from oracle import oracle as O
+
+        if O.ref_available():
+            ref = O.ref_strong_branch(lp, x, cands, 60)
+            zc, zn = ref["z"], ref["z_node"]
+            score = np.maximum(zc[:, 0] - zn, 1e-6) * np.maximum(zc[:, 1] - zn, 1e-6)
+            fin = np.isfinite(zc)
+            rel = np.abs(sb.z[fin] - zc[fin]) / (1.0 + np.abs(zc[fin]))
+            out["cpu_reference"] = {
+                "children_per_s": 2 * len(cands) / ref["seconds"], "seconds": ref["seconds"], "cores": 1,
+                "kind": "reference", "sample": "warm dual simplex per child, 60-iteration limit (the reference's "
+                "sb_iter_limit default), the whole candidate loop",
+                "statuses": {str(k): int(v) for k, v in zip(*np.unique(ref["status"], return_counts=True))},
+                "same_choice": bool(int(cands[int(np.argmax(score))]) == sb.var) if sb.action == 0 else None,
+                "max_rel_z_diff": float(rel.max()) if rel.size else None}
+            out["speedup_vs_cpu_reference"] = ref["seconds"] / t
+    return out
+
+
 def batch_measure(dist, rank: int, world: int, steps: int = 3, seq_sample: int = 24) -> dict:
     """512 random feasible LPs of log-uniform size (m in [50, 4000],
     n = 2.5 m, 4-12 nonzeros per column, seeds 1000..1511): LPs/s of the
@@ -487,6 +541,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-LP batch measurement")
     ap.add_argument("--no-diff", action="store_true", help="skip the differentiable-layer measurement")
     ap.add_argument("--no-qp", action="store_true", help="skip the portfolio-QP measurement")
+    ap.add_argument("--no-branch", action="store_true", help="skip the strong-branching measurement")
     ap.add_argument("--profile", nargs="?", const="single", choices=["single", "batch"],
                     help="short fixed sequence for ncu: 'single' = the blending LP (upload, two solves, 3 timed "
                          "iterations per level); 'batch' = the 512-LP batch (one solve, 3 timed FP32 iterations)")
@@ -604,6 +659,9 @@ def main():
     qp = None
     if not args.no_qp and rank == 0:
         qp = qp_measure()
+    branch = None
+    if not args.no_branch and rank == 0:
+        branch = branch_measure(cpu=not args.no_cpu_baseline and world == 1)
     line = None
     if rank == 0:
         cpu = None
@@ -667,6 +725,7 @@ def main():
             "batch": batch,
             "diff": diff,
             "qp": qp,
+            "strong_branching": branch,
         }
         print(json.dumps(line), flush=True)
     prob.close()

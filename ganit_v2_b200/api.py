@@ -176,6 +176,7 @@ EXPORTS = [
     "gb_diff_default_options", "gb_diff_set_options", "gb_diff_backward", "gb_diff_get_info", "gb_diff_tail_start", "gb_diff_destroy",
     "gb_eval_kkt_noalloc", "gb_read_mps", "gb_model_lp", "gb_model_name", "gb_model_free", "gb_factor_detect",
     "gb_factor_lp", "gb_factor_expand", "gb_factor_free", "gb_model_is_int", "gb_strong_branch",
+    "gb_problem_set_start", "gb_batch_set_start", "gb_batch_clear_start",
 ]
 
 _lib = None
@@ -223,7 +224,9 @@ def load_library(path: str = LIB_PATH):
         "gb_model_free": (None, [vp]), "gb_factor_detect": (i32, [vp, vp]), "gb_factor_lp": (vp, [vp]),
         "gb_factor_expand": (i32, [vp, vp, vp, vp, vp]), "gb_factor_free": (None, [vp]),
         "gb_model_is_int": (vp, [vp]),
-        "gb_strong_branch": (i32, [vp, vp, i32, vp, dbl, dbl, vp, vp, vp]),
+        "gb_strong_branch": (i32, [vp, vp, vp, i32, vp, dbl, dbl, vp, vp, vp]),
+        "gb_problem_set_start": (i32, [vp, vp, vp]), "gb_batch_set_start": (i32, [vp, i32, vp, vp]),
+        "gb_batch_clear_start": (i32, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -240,6 +243,13 @@ def _check(rc: int):
 
 def _p(a):
     return None if a is None else a.ctypes.data
+
+
+def _vec(a, k: int, name: str) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.shape != (k,):
+        raise ValueError(f"{name} must have {k} entries")
+    return a
 
 
 class _LpView:
@@ -404,21 +414,26 @@ def most_fractional(x, cols, k: int) -> np.ndarray:
 
 
 def strong_branch(lp: LP, x, candidates, node_obj: float, cutoff: float = float("inf"),
-                  opt: Options | None = None) -> StrongBranch:
+                  opt: Options | None = None, y=None) -> StrongBranch:
     """Strong-branch the candidate columns of a MILP node LP on the GPU
     (gb_strong_branch): both children of every candidate solved as one batch,
-    each with a rigorous bound from its duals.  Objectives in minimisation form."""
+    each with a rigorous bound from its duals.  Objectives in minimisation form.
+    With the node's duals ``y`` the children start from the node's point."""
     lib = load_library()
     view = _LpView(lp)
     x = np.ascontiguousarray(x, dtype=np.float64)
     cand = np.ascontiguousarray(candidates, dtype=np.int32)
     if x.shape != (lp.n,) or cand.ndim != 1 or cand.size == 0:
         raise ValueError("x must have n entries and candidates at least one")
+    if y is not None:
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        if y.shape != (lp.m,):
+            raise ValueError("y must have m entries")
     o = _opts(opt)
     out = (_GbBranchCand * cand.size)()
     dec = _GbBranchDecision()
-    _check(lib.gb_strong_branch(C.byref(view.s), _p(x), int(cand.size), _p(cand), float(node_obj), float(cutoff),
-                                C.addressof(o), out, C.byref(dec)))
+    _check(lib.gb_strong_branch(C.byref(view.s), _p(x), _p(y), int(cand.size), _p(cand), float(node_obj),
+                                float(cutoff), C.addressof(o), out, C.byref(dec)))
     return StrongBranch(
         candidates=cand.copy(),
         z=np.array([[c.z[0], c.z[1]] for c in out]),
@@ -481,6 +496,14 @@ class Problem:
         h = C.c_void_p()
         _check(self._lib.gb_problem_create(C.addressof(v.s), C.addressof(o), C.byref(h)))
         self._h = h
+
+    def set_start(self, x=None, y=None) -> None:
+        """Warm start of later solves (gb_problem_set_start): (x, y) in
+        original units, x projected onto the bounds; None / NaN entries keep
+        the default start; both None restores it."""
+        x = None if x is None else _vec(x, self.n, "x")
+        y = None if y is None else _vec(y, self.m, "y")
+        _check(self._lib.gb_problem_set_start(self._h, _p(x), _p(y)))
 
     def solve(self, opt: Options | None = None, fetch: bool = True) -> Result:
         o = _opts(opt)
@@ -580,6 +603,16 @@ class BatchSolver:
                 x, y = self.solution(i)
             out.append(_result(r, x, y))
         return out
+
+    def set_start(self, i: int, x=None, y=None) -> None:
+        """Warm start of instance i (gb_batch_set_start)."""
+        lp = self.lps[i]
+        x = None if x is None else _vec(x, lp.n, "x")
+        y = None if y is None else _vec(y, lp.m, "y")
+        _check(self._lib.gb_batch_set_start(self._h, int(i), _p(x), _p(y)))
+
+    def clear_start(self) -> None:
+        _check(self._lib.gb_batch_clear_start(self._h))
 
     def solution(self, i: int):
         lp = self.lps[i]

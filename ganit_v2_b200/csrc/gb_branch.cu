@@ -28,6 +28,11 @@
 // +inf -> node infeasible; one -> tighten the column to the other side;
 // else the largest score max(z_down - z, 1e-6) * max(z_up - z, 1e-6), the
 // first candidate winning ties.
+//
+// Given the node's duals y as well, every child starts from the node's point
+// (x, y) -- x projected onto the child's bounds -- instead of the default
+// start (an extension: the reference's PDHG always starts from the
+// projection of 0, and the dual simplex it replaces here starts warm).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -174,8 +179,8 @@ struct Child {
     int inst = -1;     // index in the batch (-1: bounds cross, not solved)
 };
 
-void strong_branch(const gb_lp& lp, const double* x, int count, const int32_t* cand, double node_obj, double cutoff,
-                   const gb_options* opt, gb_branch_cand* out, gb_branch_decision* dec) {
+void strong_branch(const gb_lp& lp, const double* x, const double* y, int count, const int32_t* cand, double node_obj,
+                   double cutoff, const gb_options* opt, gb_branch_cand* out, gb_branch_decision* dec) {
     const auto t0 = std::chrono::steady_clock::now();
     GB_REQUIRE(count >= 1 && count <= 32767, "need 1 to 32767 candidates");  // children index the grid's y dimension
     GB_REQUIRE(lp.m >= 0 && lp.n >= 1 && lp.c && lp.l && lp.u && (lp.m == 0 || (lp.a_ptr && lp.lo && lp.hi)),
@@ -188,6 +193,10 @@ void strong_branch(const gb_lp& lp, const double* x, int count, const int32_t* c
         GB_REQUIRE(j >= 0 && j < n, "candidate column out of range");
         GB_REQUIRE(std::isfinite(x[j]), "candidate value is not finite");
         GB_REQUIRE(std::floor(x[j]) != x[j], "candidate value is integral");
+    }
+    if (y) {
+        for (int j = 0; j < n; ++j) GB_REQUIRE(std::isfinite(x[j]), "node point has a non-finite entry");
+        for (int i = 0; i < lp.m; ++i) GB_REQUIRE(std::isfinite(y[i]), "node point has a non-finite entry");
     }
     // minimisation form: the reference branches on zmin() = sign * objective
     const double sign = lp.maximize ? -1.0 : 1.0;
@@ -231,6 +240,19 @@ void strong_branch(const gb_lp& lp, const double* x, int count, const int32_t* c
     std::vector<double> cert(S, -INFINITY);
     if (S > 0) {
         std::unique_ptr<Problem> P(create_problem(S, views.data(), opt));
+        if (y) {
+            // every child starts from the node's point (x projected onto the
+            // child's bounds on the device); the duals in minimisation form
+            std::vector<double> xs(static_cast<size_t>(S) * n), ys(static_cast<size_t>(S) * std::max(lp.m, 1));
+            for (int b = 0; b < S; ++b) {
+                std::copy(x, x + n, xs.begin() + static_cast<size_t>(b) * n);
+                for (int i = 0; i < lp.m; ++i) ys[static_cast<size_t>(b) * lp.m + i] = sign * y[i];
+            }
+            P->x_start.reset(xs.size());
+            P->y_start.reset(ys.size());
+            P->x_start.upload(xs.data(), xs.size(), P->stream);
+            P->y_start.upload(ys.data(), ys.size(), P->stream);
+        }
         solve_problem(*P, opt, res.data());
         bnd.clear();
         bnd.shrink_to_fit();
@@ -382,13 +404,13 @@ void strong_branch(const gb_lp& lp, const double* x, int count, const int32_t* c
 }  // namespace
 }  // namespace gb
 
-extern "C" int gb_strong_branch(const gb_lp* lp, const double* x, int32_t count, const int32_t* cand, double node_obj,
-                                double cutoff, const gb_options* opt, gb_branch_cand* out,
+extern "C" int gb_strong_branch(const gb_lp* lp, const double* x, const double* y, int32_t count, const int32_t* cand,
+                                double node_obj, double cutoff, const gb_options* opt, gb_branch_cand* out,
                                 gb_branch_decision* decision) {
     return gb::guarded([&] {
         GB_REQUIRE(lp && x && cand && out, "null argument");
         gb_options def;
         gb_default_options(&def);
-        gb::strong_branch(*lp, x, count, cand, node_obj, cutoff, opt ? opt : &def, out, decision);
+        gb::strong_branch(*lp, x, y, count, cand, node_obj, cutoff, opt ? opt : &def, out, decision);
     });
 }

@@ -794,6 +794,12 @@ void solve_problem(Problem& P, const gb_options* opt, gb_result* res) {
     k_start_point<<<elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s>>>(P.n, P.m, P.l.get(), P.u.get(),
                                                                          P.x64.get(), P.y64.get());
     P.launches += 2;
+    if (P.x_start.get()) {
+        k_warm_point<<<elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s>>>(
+            P.n, P.m, P.icol(), P.irow(), P.l.get(), P.u.get(), P.C.get(), P.R.get(), P.scal.get(),
+            P.x_start.get(), P.y_start.get(), P.x64.get(), P.y64.get());
+        P.launches += 1;
+    }
     P.results.assign(K, InstanceResult{});
     std::vector<int> ex(K, kIterLimit), done(K, 0);
     auto set_flags = [&](auto pred) {
@@ -1141,6 +1147,37 @@ void problem_stats(const Problem& P, int64_t* launches, double* bpi) {
 // ==================================================================== C ABI
 using namespace gb;
 
+namespace gb {
+// Warm start of instance `inst` (original units; NULL keeps that side's
+// default start, NaN entries too).  Applies to every later solve.
+void set_start(Problem& P, int inst, const double* x, const double* y) {
+    GB_REQUIRE(inst >= 0 && inst < P.count, "instance index out of range");
+    GB_CUDA(cudaSetDevice(P.device));
+    const int c0 = P.col_off[inst], c1 = P.col_off[inst + 1], r0 = P.row_off[inst], r1 = P.row_off[inst + 1];
+    if (x)
+        for (int j = 0; j < c1 - c0; ++j) GB_REQUIRE(!std::isinf(x[j]), "start point has an infinite entry");
+    if (y)
+        for (int i = 0; i < r1 - r0; ++i) GB_REQUIRE(!std::isinf(y[i]), "start point has an infinite entry");
+    if (!P.x_start.get()) {
+        P.x_start.reset(std::max(P.n, 1));
+        P.y_start.reset(std::max(P.m, 1));
+        // all-ones bytes are a NaN: every entry starts as "default"
+        GB_CUDA(cudaMemsetAsync(P.x_start.get(), 0xff, sizeof(double) * P.x_start.size(), P.stream));
+        GB_CUDA(cudaMemsetAsync(P.y_start.get(), 0xff, sizeof(double) * P.y_start.size(), P.stream));
+    }
+    if (x && c1 > c0)
+        GB_CUDA(cudaMemcpyAsync(P.x_start.get() + c0, x, sizeof(double) * (c1 - c0), cudaMemcpyHostToDevice, P.stream));
+    if (y && r1 > r0)
+        GB_CUDA(cudaMemcpyAsync(P.y_start.get() + r0, y, sizeof(double) * (r1 - r0), cudaMemcpyHostToDevice, P.stream));
+    GB_CUDA(cudaStreamSynchronize(P.stream));
+}
+
+void clear_start(Problem& P) {
+    P.x_start.release();
+    P.y_start.release();
+}
+}  // namespace gb
+
 struct gb_problem {
     Problem* p;
 };
@@ -1268,6 +1305,28 @@ int gb_batch_solve(gb_batch* b, const gb_options* opt, gb_result* results) {
         gb_options def;
         gb_default_options(&def);
         solve_problem(*b->p, opt ? opt : &def, results);
+    });
+}
+
+int gb_problem_set_start(gb_problem* p, const double* x, const double* y) {
+    return guarded([&] {
+        GB_REQUIRE(p != nullptr, "problem is NULL");
+        if (!x && !y) clear_start(*p->p);
+        else set_start(*p->p, 0, x, y);
+    });
+}
+
+int gb_batch_set_start(gb_batch* b, int i, const double* x, const double* y) {
+    return guarded([&] {
+        GB_REQUIRE(b != nullptr, "batch is NULL");
+        set_start(*b->p, i, x, y);
+    });
+}
+
+int gb_batch_clear_start(gb_batch* b) {
+    return guarded([&] {
+        GB_REQUIRE(b != nullptr, "batch is NULL");
+        clear_start(*b->p);
     });
 }
 

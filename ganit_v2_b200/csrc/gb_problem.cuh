@@ -113,6 +113,7 @@ struct Problem {
     std::vector<double> scal_host;
     DevBuf<double> red_partials;
     DevBuf<double> x64, y64, xr64, yr64, xo, yo;
+    DevBuf<double> x_start, y_start;      // warm start in original units (NaN: default start); empty: none
     DevBuf<double> work1, work2;          // n / m FP64 scratch
     DevBuf<double> ftx;                   // F^T x of the DPLR Hessian (2 x qk, FP64)
     VecSet<float> v32;
@@ -148,6 +149,8 @@ struct Problem {
 extern thread_local std::string g_last_error;
 Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt);
 void solve_problem(Problem& P, const gb_options* opt, gb_result* res);
+void set_start(Problem& P, int inst, const double* x, const double* y);
+void clear_start(Problem& P);
 void certify(Problem& P);  // FP64 KKT of (x64, y64) of every instance into st_host[k].kcert
 
 // Runs f, turning exceptions into the ABI's status codes (message in g_last_error).

@@ -277,6 +277,27 @@ __global__ void k_convert(long long n, const double* __restrict__ s, T* __restri
         d[i] = static_cast<T>(s[i]);
 }
 
+// Warm start (extension): the caller's point in original units, mapped by
+// the inverse of k_unscale and projected onto the scaled bounds; a NaN entry
+// keeps the default start k_start_point wrote.
+static __global__ void k_warm_point(int n, int m, const int* inst_col, const int* inst_row, const double* l,
+                                    const double* u, const double* Cs, const double* R, const double* sc,
+                                    const double* xin, const double* yin, double* x, double* y) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const double v = xin[j];
+        if (isnan(v)) continue;
+        const double xs = v / (Cs[j] * sc[static_cast<size_t>(inst_of(inst_col, j)) * kScal + S_BSCALE]);
+        x[j] = fmin(fmax(xs, l[j]), u[j]);
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        const double v = yin[i];
+        if (isnan(v)) continue;
+        const double* s = sc + static_cast<size_t>(inst_of(inst_row, i)) * kScal;
+        y[i] = s[S_SIGN] * v / (R[i] * s[S_CSCALE]);
+    }
+}
+
 // x_orig = x' C bscale, y_orig = sign y' R cscale (pdhg_impl.hpp:310-314)
 static __global__ void k_unscale(int n, int m, const int* inst_col, const int* inst_row, const double* x,
                                  const double* y, const double* Cs, const double* R, const double* sc, double* xo,

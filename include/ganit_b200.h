@@ -156,6 +156,9 @@ int gb_problem_create(const gb_lp* lp, const gb_options* opt, gb_problem** out);
 int gb_problem_solve(gb_problem* p, const gb_options* opt, gb_result* res);
 /* Copy the unscaled solution of the last solve to host buffers (either may be NULL). */
 int gb_problem_get_solution(gb_problem* p, double* x_out, double* y_out);
+/* Warm start (extension, as gb_batch_set_start): later solves start from
+ * (x, y) in original units; both NULL restores the default start. */
+int gb_problem_set_start(gb_problem* p, const double* x, const double* y);
 void gb_problem_destroy(gb_problem* p);
 /* Stream the problem's work is issued on (a cudaStream_t). */
 void* gb_problem_stream(gb_problem* p);
@@ -312,6 +315,12 @@ int gb_batch_time_kernels(gb_batch* b, int level, int iters, double* ms_primal, 
 int gb_batch_time_kernels_graph(gb_batch* b, int level, int iters, double* ms_primal, double* ms_dual,
                                 double* ms_iteration);
 void gb_batch_destroy(gb_batch* b);
+/* Warm start (extension; the reference always starts from the projection of
+ * 0 and y = 0): instance i starts every later solve from x (n_i) / y (m_i)
+ * in original units, x projected onto its bounds; a NULL side or a NaN entry
+ * keeps the default.  gb_batch_clear_start drops every start. */
+int gb_batch_set_start(gb_batch* b, int i, const double* x, const double* y);
+int gb_batch_clear_start(gb_batch* b);
 
 /* ---------------------------------------------------------------- 3c. problem files
  * Replaces ganit::read_mps (src/mps.cpp:69-272) for callers that feed the
@@ -355,6 +364,10 @@ void gb_factor_free(gb_factor* f);
  * are solved together as one gb_batch with `opt`, and each child's rigorous
  * Lagrangian lower bound is formed on the device from its duals with
  * directed rounding.  Every x[cand[k]] must be fractional; LPs only.
+ * y (may be NULL): the node's row duals (minimisation form, as x and y of a
+ * gb_solve of the node LP after negating a maximisation); given, every
+ * child starts from (x, y), x projected onto its bounds (the default start
+ * otherwise; an extension -- the reference's dual simplex starts warm).
  * Objectives are in minimisation form (a maximisation LP's are negated), and
  * node_obj / cutoff are too (cutoff = INFINITY: no incumbent).
  * Per child (index 0 = down, 1 = up), as src/mip.cpp:750-763: z = +INF when
@@ -382,8 +395,9 @@ typedef struct {
     int32_t children_solved; /* children in the batch (bounds that cross need no solve) */
     double seconds;       /* wall time of the call */
 } gb_branch_decision;
-int gb_strong_branch(const gb_lp* lp, const double* x, int32_t count, const int32_t* cand, double node_obj,
-                     double cutoff, const gb_options* opt, gb_branch_cand* out, gb_branch_decision* decision);
+int gb_strong_branch(const gb_lp* lp, const double* x, const double* y, int32_t count, const int32_t* cand,
+                     double node_obj, double cutoff, const gb_options* opt, gb_branch_cand* out,
+                     gb_branch_decision* decision);
 
 /* ---------------------------------------------------------------- 3b. differentiable solving
  * No counterpart in the reference (it differentiates run_pdhg,

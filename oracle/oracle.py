@@ -398,3 +398,31 @@ def lagrangian_bound_exact(lp, y, j: int, lo: float, hi: float) -> float:
         cands = [d[c] * F(v) for v in (l, u) if np.isfinite(v)]
         total += min(cands) if cands else F(0)
     return total  # a Fraction: compare it with floats exactly
+
+
+def ref_strong_branch(lp, x, candidates, iter_limit: int = 60) -> dict:
+    """The reference's own strong-branching loop (warm dual simplex per child,
+    src/mip.cpp:738-760) through ref_shim.cpp: z per child in its mapping,
+    simplex statuses and iterations, the node objective, and the loop's wall
+    time (the node solve before it is not timed).  Minimisation LPs."""
+    lib = _load(REF_SO)
+    a = _arrays(lp)
+    cand = np.ascontiguousarray(candidates, dtype=np.int32)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    k = int(cand.size)
+    z = np.zeros(2 * k)
+    st = np.zeros(2 * k, np.int32)
+    it = np.zeros(2 * k, np.int64)
+    zn = C.c_double(0)
+    secs = C.c_double(0)
+    f = lib.ref_strong_branch
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 8 + [C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_long] + \
+        [C.c_void_p] * 5
+    rc = f(lp.m, lp.n, _p(a["ptr"]), _p(a["idx"]), _p(a["val"]), _p(a["c"]), _p(a["l"]), _p(a["u"]), _p(a["lo"]),
+           _p(a["hi"]), float(lp.obj_const), _p(x), _p(cand), k, int(iter_limit), C.addressof(zn), _p(z), _p(st),
+           _p(it), C.addressof(secs))
+    if rc != 0:
+        raise RuntimeError(f"reference strong branching failed ({rc})")
+    return {"z": z.reshape(k, 2), "status": st.reshape(k, 2), "iterations": it.reshape(k, 2), "z_node": zn.value,
+            "seconds": secs.value}

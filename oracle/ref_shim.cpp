@@ -10,6 +10,9 @@
 //   ganit::solve_pdhg_cpu   include/ganit/pdhg.hpp:44, src/backend_cpu.cpp:160
 //   ganit::read_mps         include/ganit/lp.hpp:50,  src/mps.cpp:69
 //   ganit::DualSimplex      src/simplex.hpp:37-93
+//   the strong-branching loop of Mip::select_branch (src/mip.cpp:738-760)
+#include <chrono>
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <memory>
@@ -186,6 +189,54 @@ int ref_dual_simplex(int m, int n, const int* ptr, const int* idx, const double*
         if (status_out)
             for (int j = 0; j < n + m && j < (int)b.status.size(); ++j) status_out[j] = b.status[j];
         return static_cast<int>(st);
+    } catch (const std::exception&) {
+        return -100;
+    }
+}
+
+// Strong branching as Mip::select_branch runs it (src/mip.cpp:738-760):
+// the node LP solved once (not timed), then per candidate j and side the
+// state saved, the child's bounds set ((l_j, floor x_j) / (ceil x_j, u_j)),
+// a warm dual-simplex solve with iter_limit (< 0: to optimality), the
+// outcome recorded in the reference's mapping (Infeasible / Cutoff -> +inf,
+// Optimal -> the objective, else max(z, dual bound) or z), the state
+// restored.  Minimisation LPs.  z_out / status_out / iters_out hold 2k
+// entries (down, up per candidate); *seconds the loop's wall time.
+int ref_strong_branch(int m, int n, const int* ptr, const int* idx, const double* val, const double* c,
+                      const double* l, const double* u, const double* lo, const double* hi, double obj_const,
+                      const double* x, const int* cand, int k, long iter_limit, double* z_node, double* z_out,
+                      int* status_out, long* iters_out, double* seconds) {
+    try {
+        LP lp = make_lp(m, n, ptr, idx, val, c, l, u, lo, hi, obj_const, 0, nullptr, nullptr, nullptr);
+        DualSimplex S(lp, SimplexOptions{});
+        if (S.solve(-1, kInf) != LpStatus::Optimal) return -1;
+        const double z = S.objective();
+        *z_node = z;
+        const auto t0 = std::chrono::steady_clock::now();
+        std::unique_ptr<DualSimplex::State> saved = S.save_state();
+        for (int t = 0; t < k; ++t) {
+            const int j = cand[t];
+            const double v = x[j], cl = S.col_lower(j), cu = S.col_upper(j);
+            for (int d = 0; d < 2; ++d) {
+                const long it0 = S.iterations();
+                if (d == 0) S.set_col_bounds(j, cl, std::floor(v));
+                else S.set_col_bounds(j, std::ceil(v), cu);
+                const LpStatus st = S.solve(iter_limit, kInf);
+                double zz;
+                if (st == LpStatus::Infeasible || st == LpStatus::Cutoff) zz = kInf;
+                else if (st == LpStatus::Optimal) zz = S.objective();
+                else {
+                    const double db = S.dual_bound_min();
+                    zz = std::isfinite(db) ? std::max(z, db) : z;
+                }
+                z_out[2 * t + d] = zz;
+                status_out[2 * t + d] = static_cast<int>(st);
+                iters_out[2 * t + d] = S.iterations() - it0;
+                S.restore_state(*saved);
+            }
+        }
+        *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return 0;
     } catch (const std::exception&) {
         return -100;
     }
