@@ -7,8 +7,13 @@
 //             idx/val range with coalesced loads, stages the products
 //             val*x[idx] in shared memory, then reduces each row with a group
 //             of G lanes (G = power of two chosen from the rows per block).
-//   * LONG    one row with more than kBlockNnz nonzeros, reduced by the whole
-//             CTA (<= kLongSingle nonzeros) or
+//             A block closes before the G it would get leaves a lane of its
+//             longest row more than kMaxLaneSum products to add: one long
+//             row among many short ones (the capacity rows of a blending LP)
+//             otherwise keeps its warp -- and the CTA -- adding hundreds of
+//             products in sequence after every other row is done.
+//   * LONG    one row with more than min(kBlockNnz, 32 kMaxLaneSum)
+//             nonzeros, reduced by the whole CTA (<= kLongSingle nonzeros) or
 //   * CHUNK   a slice of a very long row: each CTA writes its partial sum to a
 //             fixed slot and the last CTA to arrive adds the slots in chunk
 //             order and runs the epilogue (no spin-waits, deterministic).
@@ -24,6 +29,8 @@
 // the resident warps.  Each row's epilogue operands are loaded before the
 // block's products are formed, so their latency overlaps the stream.
 #pragma once
+#include <algorithm>
+
 #include "gb_common.cuh"
 
 namespace gb {
@@ -31,6 +38,7 @@ namespace gb {
 constexpr int kBlockNnz = 2048;     // nonzeros per STREAM block
 constexpr int kLongSingle = 16384;  // longest row one CTA reduces alone
 constexpr int kChunkNnz = 8192;     // slice of a longer row per CTA
+constexpr int kMaxLaneSum = 32;     // STREAM: most products one lane of a row's group adds (16..64 measured)
 
 enum BlockKind : int { kStream = 0, kLong = 1, kChunk = 2 };
 
@@ -69,7 +77,7 @@ inline void schedule_rows(const int* ptr, int r_begin, int r_end, int block_nnz,
     int i = r_begin;
     while (i < r_end) {
         const int len = ptr[i + 1] - ptr[i];
-        if (len > block_nnz) {
+        if (len > block_nnz || len > 32 * kMaxLaneSum) {
             if (len <= kLongSingle) {
                 RowBlock b{};
                 b.r0 = i; b.r1 = i + 1; b.p0 = ptr[i]; b.p1 = ptr[i + 1]; b.kind = kLong; b.inst = inst;
@@ -92,7 +100,17 @@ inline void schedule_rows(const int* ptr, int r_begin, int r_end, int block_nnz,
             continue;
         }
         const int r0 = i, start = ptr[i];
-        while (i < r_end && (i - r0) < max_rows && ptr[i + 1] - start <= block_nnz) ++i;
+        int maxlen = 0;
+        while (i < r_end && (i - r0) < max_rows && ptr[i + 1] - start <= block_nnz) {
+            const int l = ptr[i + 1] - ptr[i];
+            if (i > r0) {
+                const int nr = i - r0 + 1;
+                const int g = 1 << floor_log2(std::min(32, kThreads / nr));
+                if (div_up(std::max(maxlen, l), g) > kMaxLaneSum) break;
+            }
+            maxlen = std::max(maxlen, l);
+            ++i;
+        }
         RowBlock b{};
         b.r0 = r0; b.r1 = i; b.p0 = start; b.p1 = ptr[i]; b.kind = kStream; b.inst = inst;
         const int nrows = i - r0;
