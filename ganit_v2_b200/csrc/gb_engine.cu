@@ -337,8 +337,6 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     P->red_partials.reset(kRedGrid);
     P->st.reset(count);
     GB_CUDA(cudaMemsetAsync(P->st.get(), 0, sizeof(SolveState) * count, s));
-    P->arrive.reset(1);
-    GB_CUDA(cudaMemsetAsync(P->arrive.get(), 0, sizeof(unsigned), s));
 
     // schedules (host, from the row-length histogram, per instance) and transpose
     for (int w = 0; w < 2; ++w) {
@@ -530,7 +528,6 @@ EvalArgs<M, V> eval_args(Problem& P, VecSet<V>& vs, const V* x, const V* y, int 
     a.seg_a = P.A.sched_for<M>().seg_block.get();
     a.seg_t = P.AT.sched_for<M>().seg_block.get();
     a.st = P.st.get();
-    a.arrive = P.arrive.get();
     a.partials = P.partials.get();
     a.inst_terms = P.partials.get() + static_cast<size_t>(a.A.nb + a.AT.nb) * kTerms;
     a.cond = 0;
@@ -584,10 +581,11 @@ long long capture_body(Problem& P, int ce, cudaGraphConditionalHandle cond, cuda
         launch_pdl(k_eval<M, V, 3, 3>, grid, kThreads, spmv_smem_bytes<3, V>(), s, ea);
     else
         launch_pdl(k_eval<M, V, 2, 3>, grid, kThreads, spmv_smem_bytes<3, V>(), s, ea);
+    launch_pdl(k_decide<M, V>, 1, kThreads, 0, s, ea);
     RestartArgs<V> ra{xc, yc, vs.x0.get(), vs.y0.get(), vs.xr.get(), vs.yr.get(), vs.sumx.get(), vs.sumy.get(),
                       P.n, P.m, P.icol(), P.irow(), P.st.get()};
     launch_pdl(k_restart<V>, elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s, ra);
-    nl += 2;
+    nl += 3;
     return nl;
 }
 
@@ -722,7 +720,8 @@ void run_phase(Problem& P, const gb_options* opt, double tol, int stall_exit, in
     if (P.has_q) launch_qx<M, V>(P, vs, vs.x0.get(), vs.qx.get(), s, P.launches);
     EvalArgs<M, V> ea = eval_args<M, V>(P, vs, vs.x0.get(), vs.y0.get(), kEvalInit, P.has_q);
     k_eval<M, V, 1, 1><<<ea.A.nb + ea.AT.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(ea);
-    P.launches += 1;
+    k_decide<M, V><<<1, kThreads, 0, s>>>(ea);
+    P.launches += 2;
     long long per_body = 0;
     long long bodies = 0;
     if (host_loop_mode()) {
@@ -761,7 +760,8 @@ void certify(Problem& P) {
     if (P.has_q) launch_qx<double, double>(P, vs, P.x64.get(), vs.qx.get(), s, P.launches);
     EvalArgs<double, double> ea = eval_args<double, double>(P, vs, P.x64.get(), P.y64.get(), kEvalCertify, P.has_q);
     k_eval<double, double, 1, 1><<<ea.A.nb + ea.AT.nb, kThreads, spmv_smem_bytes<1, double>(), s>>>(ea);
-    P.launches += 1;
+    k_decide<double, double><<<1, kThreads, 0, s>>>(ea);
+    P.launches += 2;
     sync_state(P);
 }
 

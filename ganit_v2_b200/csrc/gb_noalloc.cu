@@ -33,7 +33,7 @@ constexpr size_t kOffBlocks = 512;
 constexpr size_t kOffPartials = kOffBlocks + sizeof(RowBlock) * GB_NOALLOC_MAX_BLOCKS;
 constexpr size_t kOffSlots = kOffPartials + sizeof(double) * kTerms * GB_NOALLOC_MAX_BLOCKS;
 constexpr size_t kOffCounters = kOffSlots + sizeof(double) * GB_NOALLOC_MAX_SLOTS;
-constexpr size_t kOffSeg = kOffCounters + sizeof(unsigned) * GB_NOALLOC_MAX_LONG_ROWS;  // 2 x int[2] + arrive
+constexpr size_t kOffSeg = kOffCounters + sizeof(unsigned) * GB_NOALLOC_MAX_LONG_ROWS;  // 2 x int[2]
 constexpr size_t kOffTerms = kOffSeg + 64;  // the last CTA's per-instance sums (one instance)
 constexpr size_t kOffEnd = kOffTerms + sizeof(double) * kTerms;
 static_assert(kOffTerms % alignof(double) == 0, "term slot misaligned");
@@ -105,13 +105,11 @@ extern "C" int gb_eval_kkt_noalloc(const gb_scaled_lp* dev, const int32_t* h_a_p
         double* slots = reinterpret_cast<double*>(base + kOffSlots);
         unsigned* counters = reinterpret_cast<unsigned*>(base + kOffCounters);
         int* seg = reinterpret_cast<int*>(base + kOffSeg);  // A blocks [0, nbA), A^T blocks [0, nb - nbA)
-        unsigned* arrive = reinterpret_cast<unsigned*>(base + kOffSeg + 32);
         const int hseg[4] = {0, nbA, 0, nb - nbA};
         static_assert(sizeof(hseg) <= 32, "segment slot");
         GB_CUDA(cudaMemcpyAsync(blocks, g_noalloc_blocks, sizeof(RowBlock) * nb, cudaMemcpyHostToDevice, s));
         GB_CUDA(cudaMemsetAsync(counters, 0, sizeof(unsigned) * GB_NOALLOC_MAX_LONG_ROWS, s));
         GB_CUDA(cudaMemcpyAsync(seg, hseg, sizeof(hseg), cudaMemcpyHostToDevice, s));
-        GB_CUDA(cudaMemsetAsync(arrive, 0, sizeof(unsigned), s));
         SolveState h;
         std::memset(&h, 0, sizeof(h));
         h.obj_scale = sc->obj_scale;
@@ -133,12 +131,12 @@ extern "C" int gb_eval_kkt_noalloc(const gb_scaled_lp* dev, const int32_t* h_a_p
         a.count = 1;
         a.seg_a = seg;
         a.seg_t = seg + 2;
-        a.arrive = arrive;
         a.st = st;
         a.partials = partials;
         a.inst_terms = reinterpret_cast<double*>(base + kOffTerms);
         a.use_cond = 0;
         k_eval<double, double, 1, 1><<<nb, kThreads, spmv_smem_bytes<1, double>(), s>>>(a);
+        k_decide<double, double><<<1, kThreads, 0, s>>>(a);
         GB_CUDA(cudaGetLastError());
         Kkt k;
         GB_CUDA(cudaMemcpyAsync(&k, &st->kcert, sizeof(Kkt), cudaMemcpyDeviceToHost, s));

@@ -16,12 +16,14 @@
 // Every check_every iterations (pdhg_impl.hpp:142-190) one k_eval launch
 // computes, for the current iterate, the running average and the ray y - y_r,
 // all KKT pieces of pdhg_impl.hpp:92-118 in FP64 (one pass over A and one
-// over A^T, several right-hand sides per pass); its last CTA reduces each
-// instance's per-CTA partials in a fixed order and runs, one thread per
-// instance, the whole scalar decision of pdhg_impl.hpp:144-189 (convergence,
-// limits, infeasibility certificate, stall exit, adaptive restart, primal
-// weight).  k_restart applies restarts.  No host round trip happens inside a
-// precision phase.
+// over A^T, several right-hand sides per pass) as per-CTA partial sums; then
+// the one-CTA k_decide reduces each instance's partials in a fixed order and
+// runs, one thread per instance, the whole scalar decision of
+// pdhg_impl.hpp:144-189 (convergence, limits, infeasibility certificate,
+// stall exit, adaptive restart, primal weight).  The decision is a separate
+// kernel because its registers (~100 per thread) would otherwise be
+// allocated to every CTA of k_eval's grid.  k_restart applies restarts.  No
+// host round trip happens inside a precision phase.
 #pragma once
 #include "gb_spmv.cuh"
 
@@ -174,13 +176,19 @@ __global__ void __launch_bounds__(kThreads, kMinCtas<V>) k_dual(const __grid_con
 }
 
 // ---------------------------------------------------------------- KKT evaluation
-// FP64 partial sums written by every CTA of k_eval.
+// FP64 partial sums written by every CTA of k_eval: the row pass (A) forms
+// the first kRowTerms, the column pass (A^T) the rest, so a CTA carries only
+// its own pass's accumulators (register pressure sets k_eval's occupancy).
 enum Term : int {
     T_RP2_C = 0, T_RP2_A, T_ROBJ_C, T_ROBJ_A, T_ROBJ_R, T_DY2_C, T_DY2_A,
-    T_RD2_C, T_VOBJ_C, T_RD2_A, T_VOBJ_A, T_RD2_R, T_VOBJ_R, T_CX_C, T_CX_A, T_XQX_C, T_XQX_A, T_DX2_C, T_DX2_A,
-    T_UR2, T_UC2, T_CD,  // primal ray d = x - x_r: row / column recession violations^2, c'd
+    T_UR2,  // primal ray d = x - x_r: row recession violation^2
+    kRowTerms,
+    T_RD2_C = kRowTerms, T_VOBJ_C, T_RD2_A, T_VOBJ_A, T_RD2_R, T_VOBJ_R, T_CX_C, T_CX_A, T_XQX_C, T_XQX_A,
+    T_DX2_C, T_DX2_A,
+    T_UC2, T_CD,  // primal ray: column recession violation^2, c'd
     kTerms
 };
+constexpr int kColTerms = kTerms - kRowTerms;
 
 template <class M, class V>
 struct EvalArgs {
@@ -205,7 +213,6 @@ struct EvalArgs {
     const int* seg_a;            // instance k owns A blocks [seg_a[k], seg_a[k+1])
     const int* seg_t;            // and A^T blocks [seg_t[k], seg_t[k+1])
     SolveState* st;              // per instance
-    unsigned* arrive;            // CTA arrival counter (re-armed by the last CTA)
     double* partials;            // [gridDim.x][kTerms]
     double* inst_terms;          // [count][kTerms] scratch of the last CTA
     unsigned long long cond;     // cudaGraphConditionalHandle of the phase loop
@@ -262,7 +269,7 @@ template <class M, class V, int NV>
 struct EvalRowEpi {
     const EvalArgs<M, V>& a;  // kernel parameter space (__grid_constant__)
     double inv;
-    double t[kTerms];
+    double t[kRowTerms];  // indexed by the row terms
     __device__ __forceinline__ bool begin(int inst) { return eval_includes(a.st[inst], a.mode); }
     __device__ __forceinline__ static double pres2(double ax, double lo, double hi, double r) {
         double p = (ax < lo) ? lo : ax;
@@ -308,7 +315,7 @@ template <class M, class V, int NV>
 struct EvalColEpi {
     const EvalArgs<M, V>& a;  // kernel parameter space (__grid_constant__)
     double inv;
-    double t[kTerms];
+    double t[kColTerms];  // indexed by the column terms - kRowTerms
     __device__ __forceinline__ bool begin(int inst) { return eval_includes(a.st[inst], a.mode); }
     __device__ __forceinline__ static void dres(double z, double lj, double uj, double cres, double& rd2,
                                                 double& ob) {
@@ -323,24 +330,26 @@ struct EvalColEpi {
         const double cj = double(a.c[j]), lj = double(a.l[j]), uj = double(a.u[j]), cr = double(a.cres[j]);
         const V xj = a.x[j];
         const double qc = a.qx ? double(a.qx[j]) : 0.0;
-        dres(1.0 * cj - double(s[0]) + qc, lj, uj, cr, t[T_RD2_C], t[T_VOBJ_C]);
-        t[T_CX_C] += cj * double(xj);
-        if (a.qx) t[T_XQX_C] += double(xj) * qc;
+        dres(1.0 * cj - double(s[0]) + qc, lj, uj, cr, t[T_RD2_C - kRowTerms], t[T_VOBJ_C - kRowTerms]);
+        t[T_CX_C - kRowTerms] += cj * double(xj);
+        if (a.qx) t[T_XQX_C - kRowTerms] += double(xj) * qc;
         if (NV > 1) {
             const V xa = avg_of(a.sumx, j, inv);
             const V xrj = a.xr[j];
             const double qa = a.qxa ? double(a.qxa[j]) : 0.0;
-            dres(1.0 * cj - double(s[NV > 1 ? 1 : 0]) + qa, lj, uj, cr, t[T_RD2_A], t[T_VOBJ_A]);
-            dres(0.0 * cj - double(s[NV > 2 ? 2 : 0]) + 0.0, lj, uj, cr, t[T_RD2_R], t[T_VOBJ_R]);
-            t[T_CX_A] += cj * double(xa);
-            if (a.qxa) t[T_XQX_A] += double(xa) * qa;
+            dres(1.0 * cj - double(s[NV > 1 ? 1 : 0]) + qa, lj, uj, cr, t[T_RD2_A - kRowTerms],
+                 t[T_VOBJ_A - kRowTerms]);
+            dres(0.0 * cj - double(s[NV > 2 ? 2 : 0]) + 0.0, lj, uj, cr, t[T_RD2_R - kRowTerms],
+                 t[T_VOBJ_R - kRowTerms]);
+            t[T_CX_A - kRowTerms] += cj * double(xa);
+            if (a.qxa) t[T_XQX_A - kRowTerms] += double(xa) * qa;
             const double d0 = double(xj) - double(xrj), d1 = double(xa) - double(xrj);
-            t[T_DX2_C] += d0 * d0;
-            t[T_DX2_A] += d1 * d1;
+            t[T_DX2_C - kRowTerms] += d0 * d0;
+            t[T_DX2_A - kRowTerms] += d1 * d1;
             // the ray within the column's recession cone: >= 0 if l finite, <= 0 if u finite
             const double vc = (isfinite(lj) && d0 < 0 ? -d0 : 0.0) + (isfinite(uj) && d0 > 0 ? d0 : 0.0);
-            t[T_UC2] += vc * vc;
-            t[T_CD] += cj * d0;
+            t[T_UC2 - kRowTerms] += vc * vc;
+            t[T_CD - kRowTerms] += cj * d0;
         }
     }
 };
@@ -465,44 +474,49 @@ template <class M, class V, int NVA, int NVT>
 __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
     pdl_enter();
-    __shared__ double red[kWarps * kTerms];
-    __shared__ bool am_last;
+    __shared__ double red[kWarps * kColTerms];
     const int nbA = a.A.nb;
-    double t[kTerms];
+    double* part = a.partials + static_cast<size_t>(blockIdx.x) * kTerms;
     if (static_cast<int>(blockIdx.x) < nbA) {
         const double inv = avg_weight(a.st[a.A.blocks[blockIdx.x].inst], a.mode);
         EvalRowEpi<M, V, NVA> epi{a, inv, {}};
 #pragma unroll
-        for (int k = 0; k < kTerms; ++k) epi.t[k] = 0.0;
+        for (int k = 0; k < kRowTerms; ++k) epi.t[k] = 0.0;
         spmv_run<NVA, M, V>(a.A, blockIdx.x, GatherXAvg<V, NVA>{a.x, a.sumx, a.xr, inv}, epi, smem);
+        block_sum<kRowTerms>(epi.t, red);
+        if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < kTerms; ++k) t[k] = epi.t[k];
+            for (int k = 0; k < kRowTerms; ++k) part[k] = epi.t[k];
+#pragma unroll
+            for (int k = kRowTerms; k < kTerms; ++k) part[k] = 0.0;
+        }
     } else {
         const int cta = blockIdx.x - nbA;
         const double inv = avg_weight(a.st[a.AT.blocks[cta].inst], a.mode);
         EvalColEpi<M, V, NVT> epi{a, inv, {}};
 #pragma unroll
-        for (int k = 0; k < kTerms; ++k) epi.t[k] = 0.0;
+        for (int k = 0; k < kColTerms; ++k) epi.t[k] = 0.0;
         spmv_run<NVT, M, V>(a.AT, cta, GatherYAvgRay<V, NVT>{a.y, a.sumy, a.yr, inv}, epi, smem);
+        block_sum<kColTerms>(epi.t, red);
+        if (threadIdx.x == 0) {
 #pragma unroll
-        for (int k = 0; k < kTerms; ++k) t[k] = epi.t[k];
-    }
-    block_sum<kTerms>(t, red);
-    if (threadIdx.x == 0) {
+            for (int k = 0; k < kRowTerms; ++k) part[k] = 0.0;
 #pragma unroll
-        for (int k = 0; k < kTerms; ++k) a.partials[static_cast<size_t>(blockIdx.x) * kTerms + k] = t[k];
-        __threadfence();
-        const unsigned prev = atomicAdd(a.arrive, 1u);
-        am_last = (prev == gridDim.x - 1);
+            for (int k = 0; k < kColTerms; ++k) part[kRowTerms + k] = epi.t[k];
+        }
     }
-    __syncthreads();
-    if (!am_last) return;
-    // Last CTA: reduce every instance's partials in a fixed order and run its
-    // decision.  An instance with many blocks is reduced by the whole CTA
-    // (one at a time); the others by one warp each into inst_terms, after
-    // which every thread runs the decisions of its own instances (the scalar
-    // decision code is the long part, so it must not run one instance per warp).
-    __threadfence();
+}
+
+// One CTA after k_eval: reduce every instance's partials in a fixed order and
+// run its decision.  An instance with many blocks is reduced by the whole CTA
+// (one at a time); the others by one warp each into inst_terms, after which
+// every thread runs the decisions of its own instances (the scalar decision
+// code is the long part, so it must not run one instance per warp).
+template <class M, class V>
+__global__ void __launch_bounds__(kThreads) k_decide(const __grid_constant__ EvalArgs<M, V> a) {
+    pdl_enter();
+    __shared__ double red[kWarps * kTerms];
+    const int nbA = a.A.nb;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int any_active = 0;
     auto load_terms = [&](int k, int first, int step, double (&T)[kTerms]) {
@@ -563,10 +577,8 @@ __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalA
         finish(s, T);
     }
     any_active = __syncthreads_or(any_active);
-    if (threadIdx.x == 0) {
-        *a.arrive = 0u;
-        if (a.use_cond) cudaGraphSetConditional(static_cast<cudaGraphConditionalHandle>(a.cond), any_active ? 1u : 0u);
-    }
+    if (threadIdx.x == 0 && a.use_cond)
+        cudaGraphSetConditional(static_cast<cudaGraphConditionalHandle>(a.cond), any_active ? 1u : 0u);
 }
 
 // Restart / buffer bookkeeping after a check (pdhg_impl.hpp:178-185).

@@ -122,7 +122,6 @@ struct Problem {
     SolveState* st_host = nullptr;        // pinned mirror (count entries)
     DevBuf<int> phase_flags;              // per-instance flags uploaded for a phase
     int* phase_flags_host = nullptr;      // pinned
-    DevBuf<unsigned> arrive;              // k_eval arrival counter
     DevBuf<double> partials;
     std::unique_ptr<LevelGraph> graphs[4];  // levels <f32,f32>, <f32,f64>, <f64,f64>, <bf16,f32>
     double setup_seconds = 0.0;
