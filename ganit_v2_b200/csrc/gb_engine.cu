@@ -63,13 +63,6 @@ void validate_lp(const gb_lp* lp) {
     for (int i = 0; i < lp->m; ++i) GB_REQUIRE(lp->a_ptr[i + 1] >= lp->a_ptr[i], "A.ptr must be nondecreasing");
     const long long nnz = lp->a_ptr[lp->m];
     GB_REQUIRE(nnz == 0 || (lp->a_idx && lp->a_val), "missing A.idx/val");
-    int lo_idx = 0, hi_idx = 0;  // one vectorisable min / max pass instead of a branch per entry
-    for (long long p = 0; p < nnz; ++p) {
-        lo_idx = std::min(lo_idx, lp->a_idx[p]);
-        hi_idx = std::max(hi_idx, lp->a_idx[p]);
-    }
-    GB_REQUIRE(lo_idx >= 0 && (nnz == 0 || hi_idx < lp->n), "A.idx out of range");
-    for (int j = 0; j < lp->n; ++j) GB_REQUIRE(!(lp->l[j] > lp->u[j]), "column bound l > u");
     if (lp->q_rank > 0) {
         GB_REQUIRE(lp->q_F && lp->q_D, "DPLR Hessian needs q_F and q_D");
         GB_REQUIRE(lp->q_rank <= kMaxRank, "DPLR rank above 128");
@@ -81,6 +74,20 @@ void validate_lp(const gb_lp* lp) {
         const long long qn = lp->q_ptr[lp->n];
         for (long long p = 0; p < qn; ++p) GB_REQUIRE(lp->q_idx[p] >= 0 && lp->q_idx[p] < lp->n, "Q.idx out of range");
     }
+}
+
+// The entry checks of validate_lp's problem (column indices in range, l <= u):
+// the long passes, run while the upload of the same arrays is in flight and
+// before any kernel indexes with A.idx.
+void validate_entries(const gb_lp* lp) {
+    const long long nnz = lp->a_ptr[lp->m];
+    int lo_idx = 0, hi_idx = 0;  // one vectorisable min / max pass instead of a branch per entry
+    for (long long p = 0; p < nnz; ++p) {
+        lo_idx = std::min(lo_idx, lp->a_idx[p]);
+        hi_idx = std::max(hi_idx, lp->a_idx[p]);
+    }
+    GB_REQUIRE(lo_idx >= 0 && (nnz == 0 || hi_idx < lp->n), "A.idx out of range");
+    for (int j = 0; j < lp->n; ++j) GB_REQUIRE(!(lp->l[j] > lp->u[j]), "column bound l > u");
 }
 
 void upload_mat(DevMat& M, int rows, int cols, const int* ptr, const int* idx, const double* val, cudaStream_t s) {
@@ -324,6 +331,7 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     up(u0, vu, n);
     up(lo0, vlo, m);
     up(hi0, vhi, m);
+    for (int k = 0; k < count; ++k) validate_entries(&lps[k]);  // overlaps the uploads from pinned memory
     for (DevBuf<double>* b : {&P->c, &P->l, &P->u, &P->C, &P->Cres, &P->x64, &P->xr64, &P->xo, &P->work1})
         b->reset(n);
     for (DevBuf<double>* b : {&P->lo, &P->hi, &P->R, &P->Rres, &P->y64, &P->yr64, &P->yo, &P->work2}) b->reset(m);
@@ -345,7 +353,6 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     }
     P->A.sched.upload(build_schedule(P->A.host_ptr.data(), m, P->row_off.data(), count), 3, s);
     device_transpose(*P, s);
-    P->AT.sched.upload(build_schedule(P->AT.host_ptr.data(), n, P->col_off.data(), count), 3, s);
 
     // Ruiz equilibration + Pock-Chambolle (scaling.cpp:47-72); row and column
     // factors are per row / column, so the block-diagonal matrix scales every
@@ -382,6 +389,10 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     // norms of the ORIGINAL data (scaling.cpp:126-127)
     inst_reduce(*P, true, FiniteBoundSq{lo0.get(), hi0.get()}, S_BNORM, PostSqrt{}, s);
     inst_reduce(*P, false, Sq{c0.get()}, S_CNORM, PostSqrt{}, s);
+
+    // A^T's schedule, built on the host while the scaling kernels run (the
+    // power iteration is its first user)
+    P->AT.sched.upload(build_schedule(P->AT.host_ptr.data(), n, P->col_off.data(), count), 3, s);
 
     // Hessian (single problem only)
     const gb_lp& L0 = lps[0];

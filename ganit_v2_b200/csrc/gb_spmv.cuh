@@ -69,6 +69,20 @@ inline int floor_log2(int v) {
     return l;
 }
 
+// Lanes per row of a STREAM block of `nr` rows: the largest power of two
+// <= min(32, kThreads / nr) (a table: the packing loop asks once per row).
+struct LaneGroups {
+    int g[kThreads + 1];
+    constexpr LaneGroups() : g{} {
+        for (int nr = 1; nr <= kThreads; ++nr) {
+            int v = kThreads / nr < 32 ? kThreads / nr : 32, p = 1;
+            while (p * 2 <= v) p *= 2;
+            g[nr] = p;
+        }
+    }
+};
+constexpr LaneGroups kLaneGroups{};
+
 // Walks rows [r_begin, r_end) once and hands every block to `emit`; slot and
 // counter ids are numbered from *nslots / *ncounters on; blocks get `inst`.
 template <class Emit>
@@ -103,11 +117,8 @@ inline void schedule_rows(const int* ptr, int r_begin, int r_end, int block_nnz,
         int maxlen = 0;
         while (i < r_end && (i - r0) < max_rows && ptr[i + 1] - start <= block_nnz) {
             const int l = ptr[i + 1] - ptr[i];
-            if (i > r0) {
-                const int nr = i - r0 + 1;
-                const int g = 1 << floor_log2(std::min(32, kThreads / nr));
-                if (div_up(std::max(maxlen, l), g) > kMaxLaneSum) break;
-            }
+            // ceil(maxlen / g) > kMaxLaneSum  <=>  maxlen > kMaxLaneSum * g
+            if (i > r0 && std::max(maxlen, l) > kMaxLaneSum * kLaneGroups.g[i - r0 + 1]) break;
             maxlen = std::max(maxlen, l);
             ++i;
         }
