@@ -213,7 +213,7 @@ struct EvalArgs {
     const int* seg_a;            // instance k owns A blocks [seg_a[k], seg_a[k+1])
     const int* seg_t;            // and A^T blocks [seg_t[k], seg_t[k+1])
     SolveState* st;              // per instance
-    double* partials;            // [gridDim.x][kTerms]
+    double* partials;            // term-major: [kTerms][A.nb + AT.nb]; a pass writes only its own terms
     double* inst_terms;          // [count][kTerms] scratch of the last CTA
     unsigned long long cond;     // cudaGraphConditionalHandle of the phase loop
     int use_cond;                // 1 inside the loop body: the decision drives the loop
@@ -476,7 +476,8 @@ __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalA
     pdl_enter();
     __shared__ double red[kWarps * kColTerms];
     const int nbA = a.A.nb;
-    double* part = a.partials + static_cast<size_t>(blockIdx.x) * kTerms;
+    const size_t nb = static_cast<size_t>(nbA + a.AT.nb);
+    double* part = a.partials + blockIdx.x;  // term q of this CTA at part[q * nb]
     if (static_cast<int>(blockIdx.x) < nbA) {
         const double inv = avg_weight(a.st[a.A.blocks[blockIdx.x].inst], a.mode);
         EvalRowEpi<M, V, NVA> epi{a, inv, {}};
@@ -486,9 +487,7 @@ __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalA
         block_sum<kRowTerms>(epi.t, red);
         if (threadIdx.x == 0) {
 #pragma unroll
-            for (int k = 0; k < kRowTerms; ++k) part[k] = epi.t[k];
-#pragma unroll
-            for (int k = kRowTerms; k < kTerms; ++k) part[k] = 0.0;
+            for (int k = 0; k < kRowTerms; ++k) part[k * nb] = epi.t[k];
         }
     } else {
         const int cta = blockIdx.x - nbA;
@@ -500,9 +499,7 @@ __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalA
         block_sum<kColTerms>(epi.t, red);
         if (threadIdx.x == 0) {
 #pragma unroll
-            for (int k = 0; k < kRowTerms; ++k) part[k] = 0.0;
-#pragma unroll
-            for (int k = 0; k < kColTerms; ++k) part[kRowTerms + k] = epi.t[k];
+            for (int k = 0; k < kColTerms; ++k) part[(kRowTerms + k) * nb] = epi.t[k];
         }
     }
 }
@@ -522,13 +519,16 @@ __global__ void __launch_bounds__(kThreads) k_decide(const __grid_constant__ Eva
     auto load_terms = [&](int k, int first, int step, double (&T)[kTerms]) {
 #pragma unroll
         for (int q = 0; q < kTerms; ++q) T[q] = 0.0;
-        const int a0 = a.seg_a[k], a1 = a.seg_a[k + 1], t0 = a.seg_t[k], t1 = a.seg_t[k + 1];
-        const int na = a1 - a0, nt = t1 - t0;
-        for (int i = first; i < na + nt; i += step) {
-            const size_t b = i < na ? static_cast<size_t>(a0 + i) : static_cast<size_t>(nbA + t0 + i - na);
+        // row terms over the instance's A blocks, column terms over its A^T
+        // blocks; consecutive threads read consecutive blocks of one term
+        const size_t nb = static_cast<size_t>(nbA + a.AT.nb);
+        const int a0 = a.seg_a[k], a1 = a.seg_a[k + 1], t0 = nbA + a.seg_t[k], t1 = nbA + a.seg_t[k + 1];
 #pragma unroll
-            for (int q = 0; q < kTerms; ++q) T[q] += __ldcg(a.partials + b * kTerms + q);
-        }
+        for (int q = 0; q < kRowTerms; ++q)
+            for (int b = a0 + first; b < a1; b += step) T[q] += __ldcg(a.partials + q * nb + b);
+#pragma unroll
+        for (int q = kRowTerms; q < kTerms; ++q)
+            for (int b = t0 + first; b < t1; b += step) T[q] += __ldcg(a.partials + q * nb + b);
     };
     auto finish = [&](SolveState& s, const double (&T)[kTerms]) {
         s.ran_body = (a.mode == kEvalCheck) ? 1 : 0;
