@@ -195,8 +195,8 @@ void qx_dplr_f64(Problem& P, const double* x, double* out, cudaStream_t s) {
     double* part = P.partials.get();
     double* t = P.ftx.get();
     k_ftx_partial<double, 1><<<kFtxGrid, kThreads, 0, s>>>(P.n, P.qk, P.F64.get(), x, nullptr, nullptr, part);
-    k_ftx_final<<<1, kThreads, 0, s>>>(kFtxGrid, P.qk, part, t);
-    k_dplr_expand<double, 1><<<elem_grid((long long)P.n * 32, P.sms), kThreads, 0, s>>>(
+    k_ftx_final<<<P.qk, 32, 0, s>>>(kFtxGrid, part, t);
+    k_dplr_expand<double, 1><<<expand_grid(P.n), kExpandWarps * 32, expand_smem_bytes<double, 1>(P.qk), s>>>(
         P.n, P.qk, P.F64.get(), P.D64.get(), t, x, nullptr, nullptr, out, nullptr);
 }
 
@@ -231,6 +231,11 @@ void init_kernel_attrs() {
         set_smem(k_eval<float, double, 3, 3>, spmv_smem_bytes<3, double>());
         set_smem(k_eval<double, double, 3, 3>, spmv_smem_bytes<3, double>());
         set_smem(k_spmv_q2<float, double>, spmv_smem_bytes<2, double>());
+        // DPLR expansion: rows of F staged per warp, up to the largest rank
+        set_smem(k_dplr_expand<float, 1>, expand_smem_bytes<float, 1>(kMaxRank));
+        set_smem(k_dplr_expand<float, 2>, expand_smem_bytes<float, 2>(kMaxRank));
+        set_smem(k_dplr_expand<double, 1>, expand_smem_bytes<double, 1>(kMaxRank));
+        set_smem(k_dplr_expand<double, 2>, expand_smem_bytes<double, 2>(kMaxRank));
         set_smem(k_spmv_q2<double, double>, spmv_smem_bytes<2, double>());
     });
 }
@@ -486,10 +491,13 @@ void launch_qx(Problem& P, VecSet<V>& vs, const V* x, V* qx, cudaStream_t s, lon
     if (P.dplr) {
         double* part = P.partials.get();
         double* t = P.ftx.get();  // FP64 F^T x at every level
-        k_ftx_partial<V, 1><<<kFtxGrid, kThreads, 0, s>>>(P.n, P.qk, vs.F.get(), x, nullptr, nullptr, part);
-        k_ftx_final<<<1, kThreads, 0, s>>>(kFtxGrid, P.qk, part, t);
-        k_dplr_expand<V, 1><<<elem_grid((long long)P.n * 32, P.sms), kThreads, 0, s>>>(
-            P.n, P.qk, vs.F.get(), vs.D.get(), t, x, nullptr, nullptr, qx, nullptr);
+        const V* none = nullptr;
+        V* none_out = nullptr;
+        const SolveState* no_st = nullptr;
+        launch_pdl(k_ftx_partial<V, 1>, kFtxGrid, kThreads, 0, s, P.n, P.qk, vs.F.get(), x, none, no_st, part);
+        launch_pdl(k_ftx_final, P.qk, 32, 0, s, kFtxGrid, part, t);
+        launch_pdl(k_dplr_expand<V, 1>, expand_grid(P.n), kExpandWarps * 32, expand_smem_bytes<V, 1>(P.qk), s, P.n,
+                   P.qk, vs.F.get(), vs.D.get(), t, x, none, no_st, qx, none_out);
         nl += 3;
     } else {
         k_spmv<M, V><<<P.Q.sched.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(P.Q.view<M>(), x, qx);
@@ -502,10 +510,11 @@ void launch_qx2(Problem& P, VecSet<V>& vs, const V* x, cudaStream_t s, long long
     if (P.dplr) {
         double* part = P.partials.get();
         double* t = P.ftx.get();
-        k_ftx_partial<V, 2><<<kFtxGrid, kThreads, 0, s>>>(P.n, P.qk, vs.F.get(), x, vs.sumx.get(), P.st.get(), part);
-        k_ftx_final<<<1, kThreads, 0, s>>>(kFtxGrid, 2 * P.qk, part, t);
-        k_dplr_expand<V, 2><<<elem_grid((long long)P.n * 32, P.sms), kThreads, 0, s>>>(
-            P.n, P.qk, vs.F.get(), vs.D.get(), t, x, vs.sumx.get(), P.st.get(), vs.qx.get(), vs.qxa.get());
+        launch_pdl(k_ftx_partial<V, 2>, kFtxGrid, kThreads, 0, s, P.n, P.qk, vs.F.get(), x, vs.sumx.get(), P.st.get(),
+                   part);
+        launch_pdl(k_ftx_final, 2 * P.qk, 32, 0, s, kFtxGrid, part, t);
+        launch_pdl(k_dplr_expand<V, 2>, expand_grid(P.n), kExpandWarps * 32, expand_smem_bytes<V, 2>(P.qk), s, P.n,
+                   P.qk, vs.F.get(), vs.D.get(), t, x, vs.sumx.get(), P.st.get(), vs.qx.get(), vs.qxa.get());
         nl += 3;
     } else {
         k_spmv_q2<M, V><<<P.Q.sched.nb, kThreads, spmv_smem_bytes<2, V>(), s>>>(P.Q.view<M>(), x, vs.sumx.get(),

@@ -36,8 +36,8 @@
 namespace gb {
 
 constexpr int kBlockNnz = 2048;     // nonzeros per STREAM block
-constexpr int kLongSingle = 16384;  // longest row one CTA reduces alone
-constexpr int kChunkNnz = 8192;     // slice of a longer row per CTA
+constexpr int kLongSingle = 4096;   // longest row one CTA reduces alone
+constexpr int kChunkNnz = 2048;     // slice of a longer row per CTA
 constexpr int kMaxLaneSum = 32;     // STREAM: most products one lane of a row's group adds (16..64 measured)
 
 enum BlockKind : int { kStream = 0, kLong = 1, kChunk = 2 };
