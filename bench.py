@@ -234,6 +234,20 @@ def run_profile_batch():
     return 0
 
 
+def run_profile_qp():
+    """The portfolio QP for ncu: one one-shot mixed solve (launch it with
+    GANIT_B200_LAUNCH=stream so every iteration kernel is a separate launch)."""
+    import ganit_v2_b200 as gb
+    from ganit_v2_b200 import workloads as W
+
+    gb.set_device(0)
+    lp = W.portfolio_qp(100_000, 50, seed=7)
+    r = gb.solve_pdhg_gpu(lp, gb.Options(precision=gb.Precision.Mixed))
+    print(json.dumps({"profile_case": "portfolio QP, 100000 assets x 50 factors (DPLR Hessian), mixed, tol 1e-4",
+                      "status": r.status_name, "iterations": r.iterations}))
+    return 0
+
+
 def qp_measure(steps: int = 2) -> dict:
     """Convex portfolio QP: 100,000 assets, 50-factor risk model, Q = 2(FF^T + D)
     as the diagonal-plus-low-rank Hessian (workloads.portfolio_qp, seed 7),
@@ -542,14 +556,17 @@ def main():
     ap.add_argument("--no-diff", action="store_true", help="skip the differentiable-layer measurement")
     ap.add_argument("--no-qp", action="store_true", help="skip the portfolio-QP measurement")
     ap.add_argument("--no-branch", action="store_true", help="skip the strong-branching measurement")
-    ap.add_argument("--profile", nargs="?", const="single", choices=["single", "batch"],
+    ap.add_argument("--profile", nargs="?", const="single", choices=["single", "batch", "qp"],
                     help="short fixed sequence for ncu: 'single' = the blending LP (upload, two solves, 3 timed "
-                         "iterations per level); 'batch' = the 512-LP batch (one solve, 3 timed FP32 iterations)")
+                         "iterations per level); 'batch' = the 512-LP batch (one solve, 3 timed FP32 iterations); "
+                         "'qp' = the portfolio QP (one mixed solve)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.profile == "qp":
+        return run_profile_qp()
     if args.profile == "batch":
         return run_profile_batch()
     if args.profile:
