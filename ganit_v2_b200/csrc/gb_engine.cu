@@ -246,6 +246,8 @@ __global__ void k_fill_segments(const int* off, int* out) {
     for (int i = off[k] + threadIdx.x; i < off[k + 1]; i += blockDim.x) out[i] = k;
 }
 
+constexpr double kL2StreamBytes = 126.0e6;  // the B200's L2
+
 // Upload + device setup (scale_lp + estimate_norm + run_pdhg's start point)
 // of `count` instances.
 Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
@@ -436,6 +438,15 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     };
     cvt32(P->A);
     cvt32(P->AT);
+    // Matrix streams that cannot stay in L2 across iterations skip L1
+    // allocation (CsrView::nc): per-iteration bytes of the LP iteration at
+    // FP32 and at FP64 against the 126 MB L2.
+    for (int w = 0; w < 2; ++w) {
+        const double sm = w ? 8.0 : 4.0, sv = w ? 8.0 : 4.0;
+        const double iter = 2.0 * static_cast<double>(P->A.nnz) * (sm + 4.0) + 4.0 * (m + n + 2) + sv * (9.0 * n + 7.0 * m);
+        const int nc = iter > kL2StreamBytes ? 1 : 0;
+        P->A.stream_nc[w] = P->AT.stream_nc[w] = nc;
+    }
     if (P->has_q && !P->dplr) cvt32(P->Q);
     convert_data(*P, P->v32, s);
     convert_data(*P, P->v64, s);
@@ -576,9 +587,11 @@ void launch_iteration(Problem& P, VecSet<V>& vs, int k, cudaStream_t s, long lon
     iteration_args<M, V>(P, vs, k, pa, da);
     if (P.has_q) launch_qx<M, V>(P, vs, pa.x, vs.qx.get(), s, nl);
     constexpr size_t sm = spmv_smem_bytes<1, V>();
-    launch_pdl(k_primal<M, V>, pa.AT.nb, kThreads, sm, s, pa);
+    if (pa.AT.nc) launch_pdl(k_primal<M, V, true>, pa.AT.nb, kThreads, sm, s, pa);
+    else launch_pdl(k_primal<M, V>, pa.AT.nb, kThreads, sm, s, pa);
     if (mid) GB_CUDA(cudaEventRecord(mid, s));
-    launch_pdl(k_dual<M, V>, da.A.nb, kThreads, sm, s, da);
+    if (da.A.nc) launch_pdl(k_dual<M, V, true>, da.A.nb, kThreads, sm, s, da);
+    else launch_pdl(k_dual<M, V>, da.A.nb, kThreads, sm, s, da);
     nl += 2;
 }
 
@@ -1007,10 +1020,16 @@ void time_level_graph(Problem& P, int iters, double* msp, double* msd, double* m
         return static_cast<double>(ms) / iters;
     };
     *msp = timed_graph([&](cudaStream_t cs) {
-        for (int k = 0; k < iters; ++k) launch_pdl(k_primal<M, V>, pa.AT.nb, kThreads, sm, cs, pa);
+        for (int k = 0; k < iters; ++k) {
+            if (pa.AT.nc) launch_pdl(k_primal<M, V, true>, pa.AT.nb, kThreads, sm, cs, pa);
+            else launch_pdl(k_primal<M, V>, pa.AT.nb, kThreads, sm, cs, pa);
+        }
     });
     *msd = timed_graph([&](cudaStream_t cs) {
-        for (int k = 0; k < iters; ++k) launch_pdl(k_dual<M, V>, da.A.nb, kThreads, sm, cs, da);
+        for (int k = 0; k < iters; ++k) {
+            if (da.A.nc) launch_pdl(k_dual<M, V, true>, da.A.nb, kThreads, sm, cs, da);
+            else launch_pdl(k_dual<M, V>, da.A.nb, kThreads, sm, cs, da);
+        }
     });
     *msi = timed_graph([&](cudaStream_t cs) {
         long long nl = 0;

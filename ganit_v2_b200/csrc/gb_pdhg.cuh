@@ -122,12 +122,12 @@ struct PrimalEpi {
     }
 };
 
-template <class M, class V>
+template <class M, class V, bool NC = false>
 __global__ void __launch_bounds__(kThreads, kMinCtas<V>) k_primal(const __grid_constant__ PrimalArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
     pdl_enter();
     PrimalEpi<M, V> epi{&a, V(0)};
-    spmv_run<1, M, V>(a.AT, blockIdx.x, GatherOne<V>{a.y}, epi, smem);
+    spmv_run<1, M, V, NC>(a.AT, blockIdx.x, GatherOne<V>{a.y}, epi, smem);
 }
 
 template <class M, class V>
@@ -167,12 +167,12 @@ struct DualEpi {
     }
 };
 
-template <class M, class V>
+template <class M, class V, bool NC = false>
 __global__ void __launch_bounds__(kThreads, kMinCtas<V>) k_dual(const __grid_constant__ DualArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
     pdl_enter();
     DualEpi<M, V> epi{&a, V(0)};
-    spmv_run<1, M, V>(a.A, blockIdx.x, GatherOne<V>{a.xbar}, epi, smem);
+    spmv_run<1, M, V, NC>(a.A, blockIdx.x, GatherOne<V>{a.xbar}, epi, smem);
 }
 
 // ---------------------------------------------------------------- KKT evaluation

@@ -205,6 +205,16 @@ struct CsrView {
     // nonzero (allocated with padded_nnz), so STREAM blocks use 16-byte loads.
     // Views of caller-owned arrays leave it 0 (scalar loads).
     int vec = 0;
+    // 1: launch the iteration kernels' variant whose 16-byte idx / val loads
+    // skip L1 allocation (spmv_run<..., true>: ld.global.nc with
+    // L1::no_allocate), set when an iteration's data at this precision does
+    // not fit in L2 and so streams from HBM.  Measured on B200: -15% per
+    // iteration on the 512-LP batch (207 MB per FP32 iteration), neutral to
+    // +8% per kernel on the blending LP at FP64 (104 MB), +20% on it at FP32
+    // (64 MB, L2-resident); so only iterations above the L2 size switch.  A
+    // template choice, not a branch: a branch in the loop costs the
+    // 32-register kernels spills.
+    int nc = 0;
 };
 
 // Element count of idx / val arrays allocated for 16-byte loads (CsrView::vec).
@@ -226,6 +236,25 @@ __device__ __forceinline__ void load4(const double* p, double (&o)[4]) {
     const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
     o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
 }
+
+// The same 16-byte loads without L1 allocation (CsrView::nc).
+__device__ __forceinline__ int4 ld_stream(const int4* p) {
+    int4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p));
+    return v;
+}
+__device__ __forceinline__ void load4_stream(const float* p, float (&o)[4]) {
+    asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(o[0]), "=f"(o[1]), "=f"(o[2]), "=f"(o[3])
+                 : "l"(p));
+}
+__device__ __forceinline__ void load4_stream(const double* p, double (&o)[4]) {
+    asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(o[0]), "=d"(o[1]) : "l"(p));
+    asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(o[2]), "=d"(o[3]) : "l"(p + 2));
+}
+__device__ __forceinline__ void load4_stream(const __nv_bfloat16* p, __nv_bfloat16 (&o)[4]) { load4(p, o); }
 
 // Gather of a single right-hand side.
 template <class V>
@@ -334,7 +363,7 @@ __device__ __forceinline__ void reduce_rows(const RowBlock& b, const V* prod, in
 // instance that is not iterating (and loads per-instance scalars);
 // epi.prefetch(row) loads a row's epilogue operands (issued before the
 // block's products) and epi(row, const V(&)[NV], pre) consumes a finished row.
-template <int NV, class M, class V, class Gather, class Epi>
+template <int NV, class M, class V, bool NC = false, class Gather, class Epi>
 __device__ __forceinline__ void spmv_run(const CsrView<M>& A, int cta, const Gather& g, Epi& epi,
                                          unsigned char* smem) {
     V* prod = reinterpret_cast<V*>(smem);
@@ -364,9 +393,15 @@ __device__ __forceinline__ void spmv_run(const CsrView<M>& A, int cta, const Gat
         const int q0 = b.p0 >> 2, q1 = (b.p1 + 3) >> 2;
 #pragma unroll 1
         for (int q = q0 + tid; q < q1; q += kThreads) {
-            const int4 j4 = __ldg(reinterpret_cast<const int4*>(A.idx) + q);
+            int4 j4;
             M a4[4];
-            load4(A.val + 4 * q, a4);
+            if constexpr (NC) {
+                j4 = ld_stream(reinterpret_cast<const int4*>(A.idx) + q);
+                load4_stream(A.val + 4 * q, a4);
+            } else {
+                j4 = __ldg(reinterpret_cast<const int4*>(A.idx) + q);
+                load4(A.val + 4 * q, a4);
+            }
             const int js[4] = {j4.x, j4.y, j4.z, j4.w};
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
