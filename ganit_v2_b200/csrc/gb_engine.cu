@@ -409,6 +409,8 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     P->partials.reset(std::max<size_t>(static_cast<size_t>(kFtxGrid) * 2 * kMaxRank,
                                        static_cast<size_t>(P->A.sched.nb + P->AT.sched.nb + count) * kTerms));
     P->ftx.reset(2 * kMaxRank);
+    P->decide_sync.reset(2);
+    GB_CUDA(cudaMemsetAsync(P->decide_sync.get(), 0, 2 * sizeof(unsigned), s));
     P->v32.alloc(n, m, P->qk, P->has_q);
     P->v64.alloc(n, m, P->qk, P->has_q);
     if (P->has_q && !P->dplr) {
@@ -561,6 +563,7 @@ EvalArgs<M, V> eval_args(Problem& P, VecSet<V>& vs, const V* x, const V* y, int 
     a.st = P.st.get();
     a.partials = P.partials.get();
     a.inst_terms = P.partials.get() + static_cast<size_t>(a.A.nb + a.AT.nb) * kTerms;
+    a.sync = P.decide_sync.get();
     a.cond = 0;
     a.use_cond = 0;
     return a;
@@ -614,7 +617,7 @@ long long capture_body(Problem& P, int ce, cudaGraphConditionalHandle cond, cuda
         launch_pdl(k_eval<M, V, 3, 3>, grid, kThreads, spmv_smem_bytes<3, V>(), s, ea);
     else
         launch_pdl(k_eval<M, V, 2, 3>, grid, kThreads, spmv_smem_bytes<3, V>(), s, ea);
-    launch_pdl(k_decide<M, V>, 1, kThreads, 0, s, ea);
+    launch_pdl(k_decide<M, V>, decide_grid(P.count), kThreads, 0, s, ea);
     RestartArgs<V> ra{xc, yc, vs.x0.get(), vs.y0.get(), vs.xr.get(), vs.yr.get(), vs.sumx.get(), vs.sumy.get(),
                       P.n, P.m, P.icol(), P.irow(), P.st.get()};
     launch_pdl(k_restart<V>, elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s, ra);
@@ -753,7 +756,7 @@ void run_phase(Problem& P, const gb_options* opt, double tol, int stall_exit, in
     if (P.has_q) launch_qx<M, V>(P, vs, vs.x0.get(), vs.qx.get(), s, P.launches);
     EvalArgs<M, V> ea = eval_args<M, V>(P, vs, vs.x0.get(), vs.y0.get(), kEvalInit, P.has_q);
     k_eval<M, V, 1, 1><<<ea.A.nb + ea.AT.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(ea);
-    k_decide<M, V><<<1, kThreads, 0, s>>>(ea);
+    k_decide<M, V><<<decide_grid(P.count), kThreads, 0, s>>>(ea);
     P.launches += 2;
     long long per_body = 0;
     long long bodies = 0;
@@ -793,7 +796,7 @@ void certify(Problem& P) {
     if (P.has_q) launch_qx<double, double>(P, vs, P.x64.get(), vs.qx.get(), s, P.launches);
     EvalArgs<double, double> ea = eval_args<double, double>(P, vs, P.x64.get(), P.y64.get(), kEvalCertify, P.has_q);
     k_eval<double, double, 1, 1><<<ea.A.nb + ea.AT.nb, kThreads, spmv_smem_bytes<1, double>(), s>>>(ea);
-    k_decide<double, double><<<1, kThreads, 0, s>>>(ea);
+    k_decide<double, double><<<decide_grid(P.count), kThreads, 0, s>>>(ea);
     P.launches += 2;
     sync_state(P);
 }

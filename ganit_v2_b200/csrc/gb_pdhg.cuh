@@ -214,10 +214,16 @@ struct EvalArgs {
     const int* seg_t;            // and A^T blocks [seg_t[k], seg_t[k+1])
     SolveState* st;              // per instance
     double* partials;            // term-major: [kTerms][A.nb + AT.nb]; a pass writes only its own terms
-    double* inst_terms;          // [count][kTerms] scratch of the last CTA
+    double* inst_terms;          // [count][kTerms] scratch of k_decide
     unsigned long long cond;     // cudaGraphConditionalHandle of the phase loop
     int use_cond;                // 1 inside the loop body: the decision drives the loop
+    unsigned* sync = nullptr;    // k_decide over several CTAs: {arrivals, any instance active}
 };
+
+// k_decide's grid: one CTA for a single problem, else one CTA per
+// kDecideInst instances (one instance per warp while reducing).
+constexpr int kDecideInst = kWarps;
+inline int decide_grid(int count) { return count == 1 ? 1 : (count + kDecideInst - 1) / kDecideInst; }
 
 template <class V>
 __device__ __forceinline__ V avg_of(const V* s, int k, double inv) {
@@ -504,17 +510,23 @@ __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalA
     }
 }
 
-// One CTA after k_eval: reduce every instance's partials in a fixed order and
-// run its decision.  An instance with many blocks is reduced by the whole CTA
-// (one at a time); the others by one warp each into inst_terms, after which
-// every thread runs the decisions of its own instances (the scalar decision
-// code is the long part, so it must not run one instance per warp).
+// After k_eval: reduce every instance's partials in a fixed order and run its
+// decision.  A single problem is one CTA; a batch gets one CTA per
+// kDecideInst instances (decide_grid).  Within a CTA an instance with many
+// blocks is reduced by the whole CTA (one at a time); the others by one warp
+// each into inst_terms, after which every thread runs the decisions of its own
+// instances (the scalar decision code is the long part, so it must not run one
+// instance per warp).  With several CTAs the last to arrive sets the phase
+// loop's condition from the OR of every CTA's "some instance still active" and
+// re-arms the two sync words.
 template <class M, class V>
 __global__ void __launch_bounds__(kThreads) k_decide(const __grid_constant__ EvalArgs<M, V> a) {
     pdl_enter();
     __shared__ double red[kWarps * kTerms];
     const int nbA = a.A.nb;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int k0 = gridDim.x == 1 ? 0 : blockIdx.x * kDecideInst;
+    const int k1 = gridDim.x == 1 ? a.count : min(a.count, k0 + kDecideInst);
     int any_active = 0;
     auto load_terms = [&](int k, int first, int step, double (&T)[kTerms]) {
 #pragma unroll
@@ -536,7 +548,7 @@ __global__ void __launch_bounds__(kThreads) k_decide(const __grid_constant__ Eva
         any_active |= s.active;
     };
     constexpr int kWide = 128;  // blocks above which an instance gets the whole CTA
-    for (int k = 0; k < a.count; ++k) {
+    for (int k = k0; k < k1; ++k) {
         const int nblk = (a.seg_a[k + 1] - a.seg_a[k]) + (a.seg_t[k + 1] - a.seg_t[k]);
         if (nblk <= kWide) continue;
         SolveState& s = a.st[k];
@@ -550,7 +562,7 @@ __global__ void __launch_bounds__(kThreads) k_decide(const __grid_constant__ Eva
         if (threadIdx.x == 0) finish(s, T);
         __syncthreads();
     }
-    for (int k = wid; k < a.count; k += kWarps) {
+    for (int k = k0 + wid; k < k1; k += kWarps) {
         const int nblk = (a.seg_a[k + 1] - a.seg_a[k]) + (a.seg_t[k + 1] - a.seg_t[k]);
         if (nblk > kWide || !eval_includes(a.st[k], a.mode)) continue;
         double T[kTerms];
@@ -563,7 +575,7 @@ __global__ void __launch_bounds__(kThreads) k_decide(const __grid_constant__ Eva
         }
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < a.count; k += kThreads) {
+    for (int k = k0 + threadIdx.x; k < k1; k += kThreads) {
         const int nblk = (a.seg_a[k + 1] - a.seg_a[k]) + (a.seg_t[k + 1] - a.seg_t[k]);
         if (nblk > kWide) continue;
         SolveState& s = a.st[k];
@@ -577,8 +589,20 @@ __global__ void __launch_bounds__(kThreads) k_decide(const __grid_constant__ Eva
         finish(s, T);
     }
     any_active = __syncthreads_or(any_active);
-    if (threadIdx.x == 0 && a.use_cond)
-        cudaGraphSetConditional(static_cast<cudaGraphConditionalHandle>(a.cond), any_active ? 1u : 0u);
+    if (threadIdx.x != 0) return;
+    if (gridDim.x == 1) {
+        if (a.use_cond)
+            cudaGraphSetConditional(static_cast<cudaGraphConditionalHandle>(a.cond), any_active ? 1u : 0u);
+        return;
+    }
+    if (any_active) atomicOr(a.sync + 1, 1u);
+    __threadfence();
+    if (atomicAdd(a.sync, 1u) == gridDim.x - 1) {  // last CTA: every decision is written
+        __threadfence();
+        const unsigned any = atomicExch(a.sync + 1, 0u);
+        atomicExch(a.sync, 0u);
+        if (a.use_cond) cudaGraphSetConditional(static_cast<cudaGraphConditionalHandle>(a.cond), any ? 1u : 0u);
+    }
 }
 
 // Restart / buffer bookkeeping after a check (pdhg_impl.hpp:178-185).

@@ -118,6 +118,7 @@ struct Problem {
     DevBuf<double> x_start, y_start;      // warm start in original units (NaN: default start); empty: none
     DevBuf<double> work1, work2;          // n / m FP64 scratch
     DevBuf<double> ftx;                   // F^T x of the DPLR Hessian (2 x qk, FP64)
+    DevBuf<unsigned> decide_sync;         // k_decide's {arrivals, any active} (re-armed by its last CTA)
     VecSet<float> v32;
     VecSet<double> v64;
     DevBuf<SolveState> st;                // per instance
