@@ -103,3 +103,25 @@ def test_batch_with_bf16_phase_certifies_every_instance(batch, oracle_built):
                 assert abs(r.pobj - o.pobj) <= 1e-3 * (1 + abs(o.pobj))
         k = bs.time_kernels(3, 10)
         assert k["ms_primal"] > 0 and k["bytes_per_iter"] > 0
+
+
+def test_streamed_batch_is_bit_identical_to_a_cached_one():
+    """A batch whose FP32 iteration exceeds the L2 (the 512-LP batch, 207 MB)
+    runs the iteration kernels' variant that streams idx / val without L1
+    allocation; its first 48 instances, batched alone (well inside the L2),
+    run the default loads.  Loads change nothing but caching, and instances
+    of a batch never share a row block or a reduction, so every instance
+    gives the same bits either way."""
+    import ganit_v2_b200 as gb
+
+    lps = W.lp_batch(512, seed=1000)
+    opt = gb.Options(precision=gb.Precision.Mixed)
+    with gb.BatchSolver(lps, opt) as bs:
+        big = bs.solve(opt)
+    with gb.BatchSolver(lps[:48], opt) as bs:
+        small = bs.solve(opt)
+    assert all(r.status_name == "OPTIMAL" for r in big)
+    for i in range(48):
+        assert big[i].iterations == small[i].iterations, i
+        np.testing.assert_array_equal(big[i].x, small[i].x)
+        np.testing.assert_array_equal(big[i].y, small[i].y)
