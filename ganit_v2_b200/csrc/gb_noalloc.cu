@@ -34,7 +34,7 @@ constexpr size_t kOffPartials = kOffBlocks + sizeof(RowBlock) * GB_NOALLOC_MAX_B
 constexpr size_t kOffSlots = kOffPartials + sizeof(double) * kTerms * GB_NOALLOC_MAX_BLOCKS;
 constexpr size_t kOffCounters = kOffSlots + sizeof(double) * GB_NOALLOC_MAX_SLOTS;
 constexpr size_t kOffSeg = kOffCounters + sizeof(unsigned) * GB_NOALLOC_MAX_LONG_ROWS;  // 2 x int[2]
-constexpr size_t kOffTerms = kOffSeg + 64;  // the last CTA's per-instance sums (one instance)
+constexpr size_t kOffTerms = kOffSeg + 64;  // k_decide's per-instance sums (one instance)
 constexpr size_t kOffEnd = kOffTerms + sizeof(double) * kTerms;
 static_assert(kOffTerms % alignof(double) == 0, "term slot misaligned");
 static_assert(sizeof(SolveState) <= kOffBlocks, "state slot too small");
