@@ -153,8 +153,8 @@ void inst_reduce(Problem& P, bool rows, F f, int slot, Post post, cudaStream_t s
     if (P.count == 1) {
         reduce_to(s, rows ? P.m : P.n, f, P.red_partials.get(), P.scal.get() + slot, post);
     } else {
-        k_seg_red<F, Post><<<P.count, kThreads, 0, s>>>(rows ? P.d_row_off.get() : P.d_col_off.get(), f,
-                                                      P.scal.get() + slot, post);
+        launch_pdl(k_seg_red<F, Post>, P.count, kThreads, 0, s,
+                   static_cast<const int*>(rows ? P.d_row_off.get() : P.d_col_off.get()), f, P.scal.get() + slot, post);
     }
 }
 
@@ -180,12 +180,15 @@ void power_iteration(Problem& P, bool q, cudaStream_t s) {
             if (P.dplr) qx_dplr_f64(P, v, z, s);
             else k_spmv<double, double><<<P.Q.sched.nb, kThreads, sm1, s>>>(P.Q.view<double>(), v, z);
         } else {
-            k_spmv<double, double><<<P.A.sched.nb, kThreads, sm1, s>>>(P.A.view<double>(), v, w);
-            k_spmv<double, double><<<P.AT.sched.nb, kThreads, sm1, s>>>(P.AT.view<double>(), w, z);
+            launch_pdl(k_spmv<double, double>, P.A.sched.nb, kThreads, sm1, s, P.A.view<double>(),
+                       static_cast<const double*>(v), w);
+            launch_pdl(k_spmv<double, double>, P.AT.sched.nb, kThreads, sm1, s, P.AT.view<double>(),
+                       static_cast<const double*>(w), z);
         }
         inst_reduce(P, false, Sq{z}, S_PW_NORM, PostSqrt{}, s);
-        k_power_vec<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, P.icol(), sc, z, v);
-        k_power_flags<<<gi, kThreads, 0, s>>>(P.count, sc);
+        launch_pdl(k_power_vec, elem_grid(n, P.sms), kThreads, 0, s, n, P.icol(), static_cast<const double*>(sc),
+                   static_cast<const double*>(z), v);
+        launch_pdl(k_power_flags, gi, kThreads, 0, s, static_cast<int>(P.count), sc);
     }
     k_finish_norms<<<gi, kThreads, 0, s>>>(P.count, P.d_nnz_off.get(), sc, q ? 1 : 0);
 }

@@ -17,6 +17,7 @@ constexpr int kRedGrid = 592;  // 4 CTAs per SM, fixed so the summation order is
 template <class F>
 __global__ void __launch_bounds__(kThreads) k_red1(long long n, F f, double* partials) {
     __shared__ double sh[kWarps];
+    pdl_enter();
     double acc = 0.0;
     for (long long i = blockIdx.x * (long long)kThreads + threadIdx.x; i < n; i += (long long)gridDim.x * kThreads)
         acc += f(i);
@@ -28,6 +29,7 @@ __global__ void __launch_bounds__(kThreads) k_red1(long long n, F f, double* par
 template <class P>
 __global__ void __launch_bounds__(kThreads) k_red2(int np, const double* partials, double* out, P post) {
     __shared__ double sh[kWarps];
+    pdl_enter();
     double acc = 0.0;
     for (int i = threadIdx.x; i < np; i += kThreads) acc += partials[i];
     double v[1] = {acc};
@@ -61,8 +63,9 @@ struct FiniteBoundSq {  // scaling.cpp:15-24
 
 template <class F, class P>
 inline void reduce_to(cudaStream_t s, long long n, F f, double* partials, double* out, P post) {
-    k_red1<F><<<kRedGrid, kThreads, 0, s>>>(n, f, partials);
-    k_red2<P><<<1, kThreads, 0, s>>>(kRedGrid, partials, out, post);
+    launch_pdl(k_red1<F>, kRedGrid, kThreads, 0, s, n, f, partials);
+    launch_pdl(k_red2<P>, 1, kThreads, 0, s, static_cast<int>(kRedGrid), static_cast<const double*>(partials), out,
+               post);
 }
 
 // ---------------------------------------------------------------- plain SpMV (y = A x)
@@ -77,6 +80,7 @@ template <class M, class V>
 __global__ void __launch_bounds__(kThreads) k_spmv(const __grid_constant__ CsrView<M> A, const V* __restrict__ x,
                                                   V* __restrict__ y) {
     extern __shared__ __align__(16) unsigned char smem[];
+    pdl_enter();
     StoreEpi<V> epi{y};
     spmv_run<1, M, V>(A, blockIdx.x, GatherOne<V>{x}, epi, smem);
 }
@@ -152,6 +156,7 @@ __device__ __forceinline__ int inst_of(const int* map, int i) { return map ? map
 template <class F, class P>
 __global__ void __launch_bounds__(kThreads) k_seg_red(const int* off, F f, double* out, P post) {
     __shared__ double sh[kWarps];
+    pdl_enter();
     const int k = blockIdx.x;
     double acc = 0.0;
     for (int i = off[k] + threadIdx.x; i < off[k + 1]; i += kThreads) acc += f(i);
@@ -221,6 +226,7 @@ static __global__ void k_scale_dplr(int n, int k, const double* __restrict__ Cs,
 // the instance's iteration stopped or ||z|| == 0 ...
 static __global__ void k_power_vec(int n, const int* inst_col, const double* sc, const double* __restrict__ z,
                                    double* __restrict__ v) {
+    pdl_enter();
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const double* s = sc + static_cast<size_t>(inst_of(inst_col, j)) * kScal;
         const double nz = s[S_PW_NORM];
@@ -229,6 +235,7 @@ static __global__ void k_power_vec(int n, const int* inst_col, const double* sc,
 }
 // ... then lambda = ||z|| ("if (nz == 0.0) break; lambda = nz").
 static __global__ void k_power_flags(int count, double* sc) {
+    pdl_enter();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= count) return;
     double* s = sc + static_cast<size_t>(k) * kScal;
