@@ -373,10 +373,19 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     k_fill<<<elem_grid(m, P->sms), kThreads, 0, s>>>(m, 1.0, P->R.get());
     k_fill<<<elem_grid(n, P->sms), kThreads, 0, s>>>(n, 1.0, P->C.get());
     const int passes = opt->ruiz_iters + (opt->pock_chambolle ? 1 : 0);
+    // lanes per row for the maxima: the average row length, rounded up to a power of two
+    auto lanes_lg = [](long long nnz, int rows) {
+        int lg = 0;
+        while (lg < 5 && (1LL << lg) * rows < nnz) ++lg;
+        return lg;
+    };
+    const int lg_a = lanes_lg(P->A.nnz, m), lg_at = lanes_lg(P->A.nnz, n);
     for (int it = 0; it < passes; ++it) {
         const int mode = it < opt->ruiz_iters ? 0 : 1;
-        k_row_norm_factor<<<gw, kThreads, 0, s>>>(m, P->A.ptr.get(), nullptr, P->A.val64.get(), mode, rs.get());
-        k_row_norm_factor<<<gw, kThreads, 0, s>>>(n, P->AT.ptr.get(), P->perm.get(), P->A.val64.get(), mode, cs.get());
+        k_row_norm_factor<<<gw, kThreads, 0, s>>>(m, P->A.ptr.get(), nullptr, P->A.val64.get(), mode, rs.get(),
+                                                  mode == 0 ? lg_a : 5);
+        k_row_norm_factor<<<gw, kThreads, 0, s>>>(n, P->AT.ptr.get(), P->perm.get(), P->A.val64.get(), mode, cs.get(),
+                                                  mode == 0 ? lg_at : 5);
         if (P->A.nnz)
             k_apply_scaling<<<ge, kThreads, 0, s>>>(static_cast<int>(P->A.nnz), P->row_of.get(), P->A.idx.get(),
                                                     rs.get(), cs.get(), P->A.val64.get());

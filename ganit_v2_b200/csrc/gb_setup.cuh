@@ -111,22 +111,31 @@ static __global__ void k_gather_transpose(int nnz, const int* __restrict__ perm,
 
 // Per-row max |a| (mode 0) or sum |a| (mode 1) of a CSR matrix whose value of
 // entry q is val[perm ? perm[q] : q]; then the factor 1/sqrt (scaling.cpp:56-57).
+// Rows go to groups of 2^lg lanes (lg = 5: one row per warp).  The caller
+// passes lg = 5 for the sums (mode 1), whose order it fixes, and a group
+// matched to the average row length for the maxima (mode 0), which are the
+// same in any order.  Every lane of a warp runs the same rounds, so the
+// shuffles always see the whole warp.
 static __global__ void k_row_norm_factor(int rows, const int* __restrict__ ptr, const int* __restrict__ perm,
-                                  const double* __restrict__ val, int mode, double* __restrict__ fac) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+                                  const double* __restrict__ val, int mode, double* __restrict__ fac, int lg) {
+    const int G = 1 << lg, rpw = 32 >> lg;  // lanes per row, rows per warp and round
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane32 = threadIdx.x & 31;
+    const int lane = lane32 & (G - 1);
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int r = warp; r < rows; r += nw) {
+    for (int r0 = warp * rpw; r0 < rows; r0 += nw * rpw) {
+        const int r = r0 + (lane32 >> lg);
         double acc = 0.0;
-        for (int q = ptr[r] + lane; q < ptr[r + 1]; q += 32) {
-            const double a = fabs(val[perm ? perm[q] : q]);
-            acc = mode == 0 ? ((acc < a) ? a : acc) : acc + a;
+        if (r < rows) {
+            for (int q = ptr[r] + lane; q < ptr[r + 1]; q += G) {
+                const double a = fabs(val[perm ? perm[q] : q]);
+                acc = mode == 0 ? ((acc < a) ? a : acc) : acc + a;
+            }
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double t = __shfl_down_sync(0xffffffffu, acc, o);
+        for (int o = G >> 1; o > 0; o >>= 1) {
+            const double t = __shfl_down_sync(0xffffffffu, acc, o, G);
             acc = mode == 0 ? ((acc < t) ? t : acc) : acc + t;
         }
-        if (lane == 0) fac[r] = acc > 0 ? 1.0 / sqrt(acc) : 1.0;
+        if (r < rows && lane == 0) fac[r] = acc > 0 ? 1.0 / sqrt(acc) : 1.0;
     }
 }
 
