@@ -692,7 +692,18 @@ def main():
             cv, kind, cores, secs, cres = cpu_baseline_run(lp, 1)
             cpu = {"value": cv, "unit": UNIT, "cores": cores, "kind": kind,
                    "sample": f"1 full mixed-precision solve of the same blending LP on the host "
-                             f"({cres.iterations} iterations, {secs[0]:.2f} s, status {cres.status})"}
+                             f"({cres.iterations} iterations, {secs[0]:.2f} s, status {cres.status})",
+                   "solve_s": cres.solve_s, "setup_s": cres.setup_s}
+            if kind == "reference":
+                # the reference README's convention: OMP_NUM_THREADS=1
+                from oracle import oracle as O
+
+                t0 = time.perf_counter()
+                r1 = O.ref_solve(lp, threads=1, precision="mixed")
+                s1 = time.perf_counter() - t0
+                cpu["single_thread"] = {"value": 1.0 / s1, "unit": UNIT, "cores": 1, "seconds": s1,
+                                        "solve_s": r1.solve_s, "setup_s": r1.setup_s,
+                                        "iterations": r1.iterations, "status": r1.status}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_mixed_max / args.steps, "higher_is_better": True,
