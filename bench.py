@@ -248,6 +248,29 @@ def run_profile_qp():
     return 0
 
 
+def run_profile_diff():
+    """The differentiable layer for ncu: 256 LPs (workloads.diff_batch), one
+    forward (launch it with GANIT_B200_LAUNCH=stream) and one backward.  The
+    forward alone issues ~190,000 launches (PDHG to 1e-6, polishing, the
+    checkpointed tail), so bound any ncu launch list with -s / -c."""
+    import numpy as np
+
+    import ganit_v2_b200 as gb
+    from ganit_v2_b200 import workloads as W
+
+    gb.set_device(0)
+    lps = W.diff_batch(256)
+    opt = gb.Options(tol=1e-6, precision=gb.Precision.Mixed)
+    ds = gb.DiffSolver(lps, opt, tail_iters=200, ckpt_every=20)
+    rng = np.random.default_rng(3)
+    res, x, y = ds.forward(opt)
+    g = ds.backward(rng.standard_normal(int(ds.n_off[-1])), rng.standard_normal(int(ds.m_off[-1])))
+    print(json.dumps({"profile_case": "differentiable layer, 256 LPs m=500 n=1000, forward + backward",
+                      "optimal": int(sum(r.status == gb.Status.Optimal for r in res)),
+                      "grad_finite": bool(all(np.all(np.isfinite(v)) for v in g.values()))}))
+    return 0
+
+
 def qp_measure(steps: int = 2) -> dict:
     """Convex portfolio QP: 100,000 assets, 50-factor risk model, Q = 2(FF^T + D)
     as the diagonal-plus-low-rank Hessian (workloads.portfolio_qp, seed 7),
@@ -556,10 +579,11 @@ def main():
     ap.add_argument("--no-diff", action="store_true", help="skip the differentiable-layer measurement")
     ap.add_argument("--no-qp", action="store_true", help="skip the portfolio-QP measurement")
     ap.add_argument("--no-branch", action="store_true", help="skip the strong-branching measurement")
-    ap.add_argument("--profile", nargs="?", const="single", choices=["single", "batch", "qp"],
+    ap.add_argument("--profile", nargs="?", const="single", choices=["single", "batch", "qp", "diff"],
                     help="short fixed sequence for ncu: 'single' = the blending LP (upload, two solves, 3 timed "
                          "iterations per level); 'batch' = the 512-LP batch (one solve, 3 timed FP32 iterations); "
-                         "'qp' = the portfolio QP (one mixed solve)")
+                         "'qp' = the portfolio QP (one mixed solve); 'diff' = the differentiable layer "
+                         "(one forward and one backward)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -567,6 +591,8 @@ def main():
         return run_reference_arm(args)
     if args.profile == "qp":
         return run_profile_qp()
+    if args.profile == "diff":
+        return run_profile_diff()
     if args.profile == "batch":
         return run_profile_batch()
     if args.profile:
