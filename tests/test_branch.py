@@ -110,3 +110,32 @@ def test_exact_bound_at_the_simplex_duals_is_the_optimum(simplex, node):
         r = simplex.ref_dual_simplex(replace(lp, l=l, u=u, meta={}))
         b = simplex.lagrangian_bound_exact(lp, r["y"], j, lo, hi)
         assert abs(float(b) - r["objective"]) <= 1e-9 * (1 + abs(r["objective"]))
+
+
+@pytest.mark.parametrize("name", ["p0548", "lseu", "egout", "bell5"])
+def test_oracle_rule_matches_the_reference_loop_on_mip_files(simplex, gb, name):
+    """The oracle's restatement of the strong-branching loop (cold dual simplex
+    per child) against the reference's own loop (src/mip.cpp:738-760: warm
+    dual simplex from the node basis, here without an iteration limit) on the
+    LP relaxations of the reference's MIP instance files: the same child
+    optimum on every side, the same infeasible sides."""
+    import os
+
+    path = f"/root/reference/instances/mip/{name}.mps"
+    if not os.path.exists(path):
+        pytest.skip("reference instance files not present")
+    lp = gb.read_mps(path)
+    assert lp.is_int is not None and not lp.maximize
+    root = simplex.ref_dual_simplex(lp)
+    assert root["status"] == 0
+    x, z = root["x"], root["objective"]
+    cands = gb.most_fractional(x, gb.fractional(x, lp.is_int), 6)
+    if len(cands) == 0:
+        pytest.skip("integral relaxation")
+    mine = simplex.strong_branch_reference(lp, x, cands, z)
+    ref = simplex.ref_strong_branch(lp, x, cands, iter_limit=-1)
+    assert abs(ref["z_node"] - z) <= 1e-9 * (1 + abs(z))
+    inf_mine, inf_ref = ~np.isfinite(mine["z"]), ~np.isfinite(ref["z"])
+    np.testing.assert_array_equal(inf_mine, inf_ref)
+    fin = ~inf_mine
+    np.testing.assert_allclose(mine["z"][fin], ref["z"][fin], rtol=1e-9, atol=1e-9)
