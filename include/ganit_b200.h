@@ -363,11 +363,14 @@ void gb_factor_free(gb_factor* f);
  * bounds are the node's) -- down: u_j = floor(x_j), up: l_j = ceil(x_j) --
  * are solved together as one gb_batch with `opt`, and each child's rigorous
  * Lagrangian lower bound is formed on the device from its duals with
- * directed rounding.  Every x[cand[k]] must be fractional; LPs only.
+ * directed rounding.  1 <= count <= 32767; every x[cand[k]] must be finite
+ * and not integral (GB_ERR_INVALID otherwise); a Hessian gives
+ * GB_ERR_UNSUPPORTED (LPs only).
  * y (may be NULL): the node's row duals (minimisation form, as x and y of a
  * gb_solve of the node LP after negating a maximisation); given, every
- * child starts from (x, y), x projected onto its bounds (the default start
- * otherwise; an extension -- the reference's dual simplex starts warm).
+ * entry of x and y must be finite and every child starts from (x, y), x
+ * projected onto its bounds (the default start otherwise; an extension --
+ * the reference's dual simplex starts warm).
  * Objectives are in minimisation form (a maximisation LP's are negated), and
  * node_obj / cutoff are too (cutoff = INFINITY: no incumbent).
  * Per child (index 0 = down, 1 = up), as src/mip.cpp:750-763: z = +INF when
