@@ -261,12 +261,14 @@ int gb_diff2(gb_backend* b, const gb_vec* a, const gb_vec* c, double* out);
  * scratch is a fixed 4 MiB __device__ array inside the library, held on every
  * GPU that loads the library until the process exits.  Limits: at most
  * GB_NOALLOC_MAX_BLOCKS row blocks for A and A^T together (a block is <= 2048
- * nonzeros and <= 256 rows), GB_NOALLOC_MAX_SLOTS chunk slots and
- * GB_NOALLOC_MAX_LONG_ROWS rows longer than 16384 nonzeros; larger problems
- * get GB_ERR_INVALID with a message.  All calls share the array, so calls
- * whose GPU work overlaps (unordered streams or threads) race; the first call
- * on a device looks the array up (cudaGetSymbolAddress) and should come
- * before any stream capture. */
+ * nonzeros and <= 256 rows), GB_NOALLOC_MAX_SLOTS chunk slots (a row of
+ * A or A^T longer than 4096 nonzeros takes one slot per 2048 nonzeros) and
+ * GB_NOALLOC_MAX_LONG_ROWS such rows (each takes one arrival counter);
+ * larger problems get GB_ERR_INVALID with a message.  All calls share the
+ * array, so calls whose GPU work overlaps (unordered streams or threads)
+ * race; the call is synchronous (it waits on `stream` for its result); the
+ * first call on a device looks the array up (cudaGetSymbolAddress) and
+ * should come before any stream capture. */
 #define GB_NOALLOC_MAX_BLOCKS 16384
 #define GB_NOALLOC_MAX_SLOTS 8192
 #define GB_NOALLOC_MAX_LONG_ROWS 4096

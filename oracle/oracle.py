@@ -21,6 +21,12 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libganit_ref.so")
+# Checkout of the reference project (its src/ and instances/): only the
+# checker builds and the tests that read the reference's instance files use
+# it; GANIT_REF_ROOT overrides the default location.
+REF_ROOT = os.environ.get("GANIT_REF_ROOT", "/root/reference")
+REF_INSTANCES = os.path.join(REF_ROOT, "instances")
+REF_MISSING = f"reference checkout not found at {REF_ROOT} (set GANIT_REF_ROOT)"
 DROPIN_SO = os.path.join(HERE, "_ref", "libganit_dropin.so")
 
 STATUS = {0: "OPTIMAL", 1: "PRIMAL_INFEASIBLE", 2: "ITERATION_LIMIT", 3: "TIME_LIMIT", 4: "NUMERICAL_ERROR"}
@@ -79,12 +85,12 @@ def build(ref: bool = True) -> None:
     """Compile the checkers with oracle/Makefile (the reference build only
     when its sources are present on this machine)."""
     targets = ["oracle"]
-    if ref and os.path.isdir("/root/reference/src"):
+    if ref and os.path.isdir(os.path.join(REF_ROOT, "src")):
         targets.append("ref")
         lib = os.path.join(os.path.dirname(HERE), "ganit_v2_b200", "libganit_b200.so")
         if os.path.exists(lib):
             targets.append("dropin")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={REF_ROOT}"] + targets, check=True)
 
 
 _libs: dict = {}
@@ -180,6 +186,23 @@ def plain_iterations(A, AT, c, l, u, lo, hi, tau, sigma, iters, x0, y0):
     f(A.rows, A.cols, _p(A.ptr), _p(A.idx), _p(A.val), _p(AT.ptr), _p(AT.idx), _p(AT.val),
       *[_p(v) for v in arr], float(tau), float(sigma), int(iters), _p(x), _p(y))
     return x, y
+
+
+def eval_kkt(A, AT, c, l, u, lo, hi, rres, cres, x, y, obj_scale, obj_const, bnorm, cnorm) -> dict:
+    """FP64 KKT of (x, y) on an already-scaled LP (ora_eval_kkt,
+    pdhg_impl.hpp:92-109 over backend_cpu.cpp:101-149)."""
+    lib = _load(ORACLE_SO)
+    f = lib.ora_eval_kkt
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 17
+    vecs = [np.ascontiguousarray(v, dtype=np.float64) for v in (c, l, u, lo, hi, rres, cres, x, y)]
+    ints = [np.ascontiguousarray(v, dtype=np.int32) for v in (A.ptr, A.idx, AT.ptr, AT.idx)]
+    vals = [np.ascontiguousarray(v, dtype=np.float64) for v in (A.val, AT.val)]
+    sc = np.array([obj_scale, obj_const, bnorm, cnorm], dtype=np.float64)
+    out = np.zeros(6)
+    f(A.rows, A.cols, _p(ints[0]), _p(ints[1]), _p(vals[0]), _p(ints[2]), _p(ints[3]), _p(vals[1]),
+      *[_p(v) for v in vecs], _p(sc), _p(out))
+    return dict(zip(("pobj", "dobj", "rel_p", "rel_d", "rel_gap", "err"), (float(v) for v in out)))
 
 
 # ---------------------------------------------------------------- reference build

@@ -487,3 +487,50 @@ int ora_plain_iterations(int m, int n, const int* a_ptr, const int* a_idx, const
     free(aty); free(xn); free(xbar); free(axbar);
     return 0;
 }
+
+/* FP64 KKT of a point (x, y) of an already-scaled LP: the eval lambda of
+ * pdhg_phase (pdhg_impl.hpp:92-109) over the reductions of backend_cpu.cpp:
+ * primal_res2 (101-112), dual_res (113-131), row_dual_obj (132-142) and
+ * dot_c (143-149), every sum taken in index order.  LPs only.
+ * sc[0..3] = obj_scale, obj_const, bnorm, cnorm; out[0..5] = pobj, dobj,
+ * rel_p, rel_d, rel_gap, err. */
+int ora_eval_kkt(int m, int n, const int* a_ptr, const int* a_idx, const double* a_val, const int* at_ptr,
+                 const int* at_idx, const double* at_val, const double* c, const double* l, const double* u,
+                 const double* lo, const double* hi, const double* rres, const double* cres, const double* x,
+                 const double* y, const double* sc, double* out) {
+    double rp2 = 0.0, rd2 = 0.0, vobj = 0.0, robj = 0.0, cx = 0.0;
+    for (int i = 0; i < m; ++i) {
+        double a = 0.0;
+        for (int p = a_ptr[i]; p < a_ptr[i + 1]; ++p) a += a_val[p] * x[a_idx[p]];
+        double pr = (a < lo[i]) ? lo[i] : a;
+        pr = (hi[i] < pr) ? hi[i] : pr;
+        double r = (a - pr) / rres[i];
+        rp2 += r * r;
+    }
+    for (int j = 0; j < n; ++j) {
+        double t = 0.0;
+        for (int p = at_ptr[j]; p < at_ptr[j + 1]; ++p) t += at_val[p] * y[at_idx[p]];
+        double z = c[j] - t + 0.0, r = 0.0;
+        if (z > 0) { if (isfinite(l[j])) vobj += z * l[j]; else r = z; }
+        else if (z < 0) { if (isfinite(u[j])) vobj += z * u[j]; else r = z; }
+        r /= cres[j];
+        rd2 += r * r;
+    }
+    for (int i = 0; i < m; ++i) {
+        if (y[i] > 0 && isfinite(lo[i])) robj += y[i] * lo[i];
+        else if (y[i] < 0 && isfinite(hi[i])) robj += y[i] * hi[i];
+    }
+    for (int j = 0; j < n; ++j) cx += c[j] * x[j];
+    const double pobj = cx * sc[0] + sc[1];
+    const double dobj = (robj + vobj) * sc[0] + sc[1];
+    const double rel_p = sqrt(rp2) / (1.0 + sc[2]);
+    const double rel_d = sqrt(rd2) / (1.0 + sc[3]);
+    const double rel_gap = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
+    out[0] = pobj;
+    out[1] = dobj;
+    out[2] = rel_p;
+    out[3] = rel_d;
+    out[4] = rel_gap;
+    out[5] = sqrt(rel_p * rel_p + rel_d * rel_d + rel_gap * rel_gap);
+    return 0;
+}

@@ -89,6 +89,15 @@ int ora_plain_iterations(int m, int n, const int* a_ptr, const int* a_idx, const
                          const double* l, const double* u, const double* lo, const double* hi, double tau,
                          double sigma, long iters, double* x, double* y);
 
+/* FP64 KKT of a point (x, y) of an already-scaled LP (pdhg_impl.hpp:92-109
+ * over backend_cpu.cpp:101-149): sc = {obj_scale, obj_const, bnorm, cnorm};
+ * out = {pobj, dobj, rel_p, rel_d, rel_gap, err}.  Checks the device KKT
+ * evaluations. */
+int ora_eval_kkt(int m, int n, const int* a_ptr, const int* a_idx, const double* a_val, const int* at_ptr,
+                 const int* at_idx, const double* at_val, const double* c, const double* l, const double* u,
+                 const double* lo, const double* hi, const double* rres, const double* cres, const double* x,
+                 const double* y, const double* sc, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -7,12 +7,16 @@ OMP_NUM_THREADS=1 and records its results:
 * synthetic instances (seeded generators of ganit_v2_b200.workloads): the
   problem arrays go to ``<name>.npz`` together with the reference's x and y,
   the scalar results to ``golden.json``;
-* the reference's own Netlib / QP instances (read with the reference MPS
-  reader from its instances/ directory): scalar results only, under
-  ``golden.json["reference_instances"]`` (their data is not copied here).
+* the reference's own Netlib / QP instances: read with the reference's MPS
+  reader (src/mps.cpp) from its instances/ directory; the parsed arrays go to
+  ``instances/<name>.npz`` (so GPU tests run where no reference checkout
+  exists) and the scalar results to ``golden.json["reference_instances"]``.
 
-Usage (in a container that has the reference checked out):
-    python tests/golden/make_golden.py [--ref-root /root/reference]
+Usage (in a container that has the reference checked out; GANIT_REF_ROOT or
+--ref-root names the checkout):
+    python tests/golden/make_golden.py            # everything
+    python tests/golden/make_golden.py --instances-only [--recompute]
+        # instance arrays; results only for instances golden.json lacks
 """
 from __future__ import annotations
 
@@ -46,8 +50,14 @@ SYNTHETIC = {
     "rand_max": (None, {}),  # maximisation variant of rand_small, built below
 }
 
-REFERENCE_INSTANCES = ["afiro", "adlittle", "bgetam", "etamacro", "shell", "25fv47", "qp/port_tiny",
-                       "qp/port_small", "qp/qblend_small"]
+REFERENCE_INSTANCES = ["afiro", "adlittle", "bgetam", "etamacro", "shell", "25fv47", "stair", "greenbea",
+                       "qp/port_tiny", "qp/port_small", "qp/qblend_small"]
+INSTANCE_DIR = os.path.join(HERE, "instances")
+
+
+def instance_path(inst: str) -> str:
+    """Fixture of a reference instance (qp/port_tiny -> instances/qp_port_tiny.npz)."""
+    return os.path.join(INSTANCE_DIR, inst.replace("/", "_") + ".npz")
 
 
 def lp_digest(lp: LP) -> str:
@@ -87,12 +97,46 @@ def result_dict(r) -> dict:
                 y_norm=float(np.linalg.norm(r.y)))
 
 
+def reference_instances(ref_root: str, known: dict, recompute: bool) -> dict:
+    """Parse every reference instance with the reference reader, write its
+    arrays, and solve it with the reference (double and mixed) unless `known`
+    already holds its results for the same data."""
+    os.makedirs(INSTANCE_DIR, exist_ok=True)
+    out = {}
+    for inst in REFERENCE_INSTANCES:
+        path = os.path.join(ref_root, "instances", inst + ".mps")
+        lp = O.ref_read_mps(path)
+        save_lp(instance_path(inst), lp, {})
+        entry = {"m": lp.m, "n": lp.n, "nnz": lp.A.nnz, "digest": lp_digest(lp), "results": {}}
+        old = known.get(inst)
+        if old is not None and old["digest"] == entry["digest"] and not recompute:
+            out[inst] = old
+            continue
+        for prec in ("double", "mixed"):
+            r = O.ref_solve(lp, threads=1, precision=prec)
+            entry["results"][prec] = result_dict(r)
+            print(f"{inst:18s} {prec:8s} {r.status:18s} it={r.iterations:6d} pobj={r.pobj:.10g}", flush=True)
+        out[inst] = entry
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default="/root/reference")
+    ap.add_argument("--ref-root", default=O.REF_ROOT)
+    ap.add_argument("--instances-only", action="store_true")
+    ap.add_argument("--recompute", action="store_true")
     a = ap.parse_args()
     O.build(ref=True)
     O._set_omp_threads(1)
+    gpath = os.path.join(HERE, "golden.json")
+    if a.instances_only:
+        with open(gpath) as f:
+            out = json.load(f)
+        out["reference_instances"] = reference_instances(a.ref_root, out.get("reference_instances", {}),
+                                                         a.recompute)
+        with open(gpath, "w") as f:
+            json.dump(out, f, indent=1, sort_keys=True)
+        return
     out = {"generator": "tests/golden/make_golden.py", "reference": "ganit::solve_pdhg_cpu, OMP_NUM_THREADS=1",
            "synthetic": {}, "reference_instances": {}}
     lps = {}
@@ -114,16 +158,8 @@ def main():
             print(f"{name:18s} {prec:8s} {r.status:18s} it={r.iterations:6d} pobj={r.pobj:.10g}")
         save_lp(os.path.join(HERE, f"{name}.npz"), lp, extra)
         out["synthetic"][name] = entry
-    for inst in REFERENCE_INSTANCES:
-        path = os.path.join(a.ref_root, "instances", inst + ".mps")
-        lp = O.ref_read_mps(path)
-        entry = {"m": lp.m, "n": lp.n, "nnz": lp.A.nnz, "digest": lp_digest(lp), "results": {}}
-        for prec in ("double", "mixed"):
-            r = O.ref_solve(lp, threads=1, precision=prec)
-            entry["results"][prec] = result_dict(r)
-            print(f"{inst:18s} {prec:8s} {r.status:18s} it={r.iterations:6d} pobj={r.pobj:.10g}")
-        out["reference_instances"][inst] = entry
-    with open(os.path.join(HERE, "golden.json"), "w") as f:
+    out["reference_instances"] = reference_instances(a.ref_root, {}, True)
+    with open(gpath, "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)
 
 

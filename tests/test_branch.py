@@ -121,9 +121,11 @@ def test_oracle_rule_matches_the_reference_loop_on_mip_files(simplex, gb, name):
     optimum on every side, the same infeasible sides."""
     import os
 
-    path = f"/root/reference/instances/mip/{name}.mps"
+    from oracle.oracle import REF_INSTANCES, REF_MISSING
+
+    path = os.path.join(REF_INSTANCES, "mip", f"{name}.mps")
     if not os.path.exists(path):
-        pytest.skip("reference instance files not present")
+        pytest.skip(REF_MISSING)
     lp = gb.read_mps(path)
     assert lp.is_int is not None and not lp.maximize
     root = simplex.ref_dual_simplex(lp)

@@ -7,7 +7,7 @@ import pytest
 
 from ganit_v2_b200 import workloads as W
 
-REF_ROOT = "/root/reference/instances"
+from oracle.oracle import REF_INSTANCES as REF_ROOT, REF_MISSING  # noqa: E402
 
 
 @pytest.fixture(scope="module")
@@ -53,7 +53,7 @@ def test_expand_restores_factors_and_row_duals(gb):
 def test_reference_portfolio_files_are_detected(gb, name):
     path = os.path.join(REF_ROOT, "qp", name)
     if not os.path.exists(path):
-        pytest.skip("reference instances not present")
+        pytest.skip(REF_MISSING)
     lp = gb.read_mps(path)
     ff = gb.FactorForm(lp)
     assert ff.factors > 0 and ff.lp.n == lp.n - ff.factors and ff.lp.m == lp.m - ff.factors

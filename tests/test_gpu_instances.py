@@ -1,0 +1,53 @@
+"""The fused B200 solver on the reference's own instance files (Netlib LPs and
+the QP set of its instances/ directory), parsed by the reference's MPS reader
+into tests/golden/instances/*.npz by make_golden.py.
+
+Bar, against the reference CPU PDHG run on the same files (golden.json
+"reference_instances", OMP_NUM_THREADS=1): the same verdict; OPTIMAL results
+FP64-certified within tol; objective within 10 * tol relative; at FP64 the
+iteration count within two KKT checks.  Published pins checked on the GPU
+result itself: bgetam is PRIMAL_INFEASIBLE after 4736 iterations
+(results.csv:2, README.md:84) and afiro's objective is -464.78 (README.md:83)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from tests.golden.make_golden import instance_path, load_lp
+from tests.test_gpu_solve import check_against
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+with open(os.path.join(GOLD, "golden.json")) as f:
+    INSTANCES = json.load(f)["reference_instances"]
+
+
+@pytest.fixture(scope="module")
+def gb():
+    import ganit_v2_b200 as gb
+
+    gb.load_library()
+    return gb
+
+
+@pytest.mark.parametrize("inst", sorted(INSTANCES))
+@pytest.mark.parametrize("prec", ["double", "mixed"])
+def test_reference_instance(gb, inst, prec):
+    lp, _ = load_lp(instance_path(inst))
+    assert (lp.m, lp.n, lp.A.nnz) == (INSTANCES[inst]["m"], INSTANCES[inst]["n"], INSTANCES[inst]["nnz"])
+    P = {"double": gb.Precision.Double, "mixed": gb.Precision.Mixed}[prec]
+    r = gb.solve_pdhg_gpu(lp, gb.Options(precision=P))
+    check_against(r, INSTANCES[inst]["results"][prec], 1e-4, prec)
+    assert np.all(np.isfinite(r.x)) and np.all(np.isfinite(r.y))
+
+
+def test_published_pins_on_the_gpu(gb):
+    lp, _ = load_lp(instance_path("bgetam"))
+    r = gb.solve_pdhg_gpu(lp, gb.Options(precision=gb.Precision.Double))
+    assert r.status_name == "PRIMAL_INFEASIBLE"
+    assert abs(r.iterations - 4736) <= 128, r.iterations
+    lp, _ = load_lp(instance_path("afiro"))
+    r = gb.solve_pdhg_gpu(lp, gb.Options(precision=gb.Precision.Double))
+    assert r.status_name == "OPTIMAL" and abs(r.pobj + 464.7853) <= 1e-4 * 464.7853 * 10
+

@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-REF_ROOT = "/root/reference/instances"
+from oracle.oracle import REF_INSTANCES as REF_ROOT, REF_MISSING  # noqa: E402
 
 
 def _files():
@@ -31,7 +31,7 @@ def gb():
 @pytest.mark.parametrize("path", _files() or ["<no reference instances>"], ids=lambda p: os.path.basename(p))
 def test_matches_the_reference_reader(gb, oracle_built, path):
     if not os.path.exists(path) or not oracle_built.ref_available():
-        pytest.skip("reference build or instances not present")
+        pytest.skip(REF_MISSING)
     a = gb.read_mps(path)
     b = oracle_built.ref_read_mps(path)
     assert (a.m, a.n, a.maximize) == (b.m, b.n, b.maximize)

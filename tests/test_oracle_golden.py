@@ -10,11 +10,20 @@ import os
 import numpy as np
 import pytest
 
-from tests.golden.make_golden import PRECISIONS, load_lp, lp_digest
+from tests.golden.make_golden import PRECISIONS, instance_path, load_lp, lp_digest
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 with open(os.path.join(GOLD, "golden.json")) as f:
     GOLDEN = json.load(f)
+
+
+@pytest.mark.parametrize("inst", sorted(GOLDEN["reference_instances"]))
+def test_instance_fixture_is_the_reference_reader_output(inst):
+    """tests/golden/instances/*.npz hold exactly what the reference's MPS
+    reader (src/mps.cpp) parsed from its instance files: the digest recorded
+    when the reference solved them."""
+    lp, _ = load_lp(instance_path(inst))
+    assert lp_digest(lp) == GOLDEN["reference_instances"][inst]["digest"]
 
 
 @pytest.mark.parametrize("name", sorted(GOLDEN["synthetic"]))
@@ -37,10 +46,10 @@ def test_oracle_matches_reference_fixture(oracle_built, name, prec):
     np.testing.assert_array_equal(r.y, arr[f"y_{prec}"])
 
 
-REF_ROOT = "/root/reference/instances"
+from oracle.oracle import REF_INSTANCES as REF_ROOT, REF_MISSING  # noqa: E402
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_ROOT), reason="reference instances not on this machine")
+@pytest.mark.skipif(not os.path.isdir(REF_ROOT), reason=REF_MISSING)
 @pytest.mark.parametrize("inst", sorted(GOLDEN["reference_instances"]))
 def test_oracle_on_reference_instances(oracle_built, inst):
     O = oracle_built
