@@ -23,7 +23,10 @@ time = max over ranks).
 
 ``--impl reference`` times the reference's own CPU implementation
 (ganit::solve_pdhg_cpu, oracle/_ref/libganit_ref.so built from the reference
-sources) with all host threads, on rank 0 only.
+sources) with all host threads, on rank 0 only.  The default arm also times
+the reference's own CUDA backend (ganit::solve_pdhg_gpu, built unmodified for
+sm_100a into oracle/_ref/libganit_refcuda.so) on the same LP and GPU
+(``reference_cuda``).
 """
 from __future__ import annotations
 
@@ -54,6 +57,8 @@ def workload():
 
 WORKLOAD_DESC = ("multi-period blending LP, 60 crudes x 16 products x 5 specs x 365 periods "
                  "(m=57305, n=405880, nnz=2886344), tol 1e-4, mixed L1->L3 with FP64 certification")
+# The same config object on both arms (the reference arm solves the same LP with the same options).
+CONFIG = {"workload": WORKLOAD_DESC, "precision": "mixed (FP32 matrix+iterates, FP64 finish/certify)"}
 
 
 def measured_peaks():
@@ -177,7 +182,7 @@ def run_reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC, "parallelism": "cpu-openmp" if kind == "reference" else "cpu-1-thread"},
+        "config": dict(CONFIG), "parallelism": "cpu-openmp" if kind == "reference" else "cpu-1-thread",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": f"{args.steps} full mixed-precision solves of the blending LP "
                                    f"({res.iterations} iterations, status {res.status})"},
@@ -186,6 +191,32 @@ def run_reference_arm(args):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def refcuda_measure(lp, steps: int = 2) -> dict:
+    """The reference's own CUDA backend (ganit::solve_pdhg_gpu of
+    src/backend_cuda.cu, unmodified, built for sm_100a into
+    oracle/_ref/libganit_refcuda.so) on the same LP and options on this GPU:
+    wall time of the whole call (host scaling, uploads, the solve with its
+    blocking reductions, unscaling), best of `steps` after one warm-up."""
+    from oracle import oracle as O
+
+    if not O.refcuda_available():
+        return {"unavailable": "oracle/_ref/libganit_refcuda.so not built (needs the reference sources)"}
+    try:
+        O.refcuda_solve(lp, precision="mixed")
+        secs, res = [], None
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            res = O.refcuda_solve(lp, precision="mixed")
+            secs.append(time.perf_counter() - t0)
+    except Exception as e:  # a failing reference leg must not hide the rest of the line
+        return {"unavailable": f"reference solve_pdhg_gpu failed: {e}"}
+    return {"solves_per_s": 1.0 / min(secs), "seconds": min(secs), "solve_s": res.solve_s, "setup_s": res.setup_s,
+            "status": res.status, "iterations": res.iterations, "fp32_iterations": res.fp32_iterations,
+            "pobj": res.pobj, "rel_p": res.rel_p, "rel_d": res.rel_d, "rel_gap": res.rel_gap,
+            "source": "src/backend_cuda.cu:382-393 (thread/warp-per-row SpMV, atomicAdd reductions read back "
+                      "per call), built with nvcc -O3 -DNDEBUG for sm_100a"}
 
 
 def run_profile_case():
@@ -356,14 +387,14 @@ def branch_measure(cpu: bool, steps: int = 3, candidates: int = 32) -> dict:
     return out
 
 
-def batch_measure(dist, rank: int, world: int, steps: int = 3, seq_sample: int = 24) -> dict:
+def batch_measure(dist, rank: int, world: int, steps: int = 3) -> dict:
     """512 random feasible LPs of log-uniform size (m in [50, 4000],
     n = 2.5 m, 4-12 nonzeros per column, seeds 1000..1511): LPs/s of the
     batched mixed-precision solver (every result FP64-certified) against the
-    plain FP64 single-instance path on the same GPU, looping over the first
-    `seq_sample` instances one by one (each resident beforehand).  Row-split
-    schedules come from the autotuner.  With N ranks the instances are split
-    by the nnz-balanced partition (no exchange; time = max over ranks)."""
+    plain FP64 single-instance path on the same GPU, looping over all 512
+    instances one by one (each resident beforehand).  Row-split schedules come
+    from the autotuner.  With N ranks the instances are split by the
+    nnz-balanced partition (no exchange; time = max over ranks)."""
     import torch
 
     import ganit_v2_b200 as gb
@@ -410,13 +441,13 @@ def batch_measure(dist, rank: int, world: int, steps: int = 3, seq_sample: int =
     it_max = reduce_max(dist, max(r.iterations for r in res))
     seq_lps = None
     if rank == 0:
-        probs = [gb.Problem(lp, fp64) for lp in lps[:seq_sample]]
+        probs = [gb.Problem(lp, fp64) for lp in lps]
         for p in probs[:2]:
             p.solve(fp64, fetch=False)
         t0 = time.perf_counter()
         for p in probs:
             p.solve(fp64, fetch=False)
-        seq_lps = seq_sample / (time.perf_counter() - t0)
+        seq_lps = len(probs) / (time.perf_counter() - t0)
         for p in probs:
             p.close()
     peak, peak_kind = measured_peaks()
@@ -433,7 +464,7 @@ def batch_measure(dist, rank: int, world: int, steps: int = 3, seq_sample: int =
             "optimal": int(n_opt), "certified_1e-4": int(certified), "iterations_max": int(it_max),
             "iterations_mean_rank0": float(np.mean([r.iterations for r in res])),
             "fp64_single_instance_loop_lps_per_s": seq_lps,
-            "fp64_loop_sample": f"first {seq_sample} instances solved one by one (FP64, resident)",
+            "fp64_loop_sample": "all 512 instances solved one by one (FP64, each resident beforehand)",
             "speedup_vs_fp64_loop": (batch_lps / seq_lps) if seq_lps else None,
             "iteration_kernels": {"bound": "hbm", "ms_primal_f32": kt["ms_primal"], "ms_dual_f32": kt["ms_dual"],
                                   "ms_per_iter_f32": it_ms, "bytes_per_iter_f32": kt["bytes_per_iter"],
@@ -579,6 +610,8 @@ def main():
     ap.add_argument("--no-diff", action="store_true", help="skip the differentiable-layer measurement")
     ap.add_argument("--no-qp", action="store_true", help="skip the portfolio-QP measurement")
     ap.add_argument("--no-branch", action="store_true", help="skip the strong-branching measurement")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip timing the reference's own CUDA backend on the headline LP")
     ap.add_argument("--profile", nargs="?", const="single", choices=["single", "batch", "qp", "diff"],
                     help="short fixed sequence for ncu: 'single' = the blending LP (upload, two solves, 3 timed "
                          "iterations per level); 'batch' = the 512-LP batch (one solve, 3 timed FP32 iterations); "
@@ -711,6 +744,12 @@ def main():
     branch = None
     if not args.no_branch and rank == 0:
         branch = branch_measure(cpu=not args.no_cpu_baseline and world == 1)
+    refcuda = None
+    if not args.no_reference_cuda and rank == 0:
+        refcuda = refcuda_measure(lp)
+        if "solves_per_s" in refcuda:
+            refcuda["value_over_reference_cuda"] = value / refcuda["solves_per_s"]
+            refcuda["e2e_over_reference_cuda"] = e2e_value / refcuda["solves_per_s"]
     line = None
     if rank == 0:
         cpu = None
@@ -736,9 +775,8 @@ def main():
             "scaling": "weak", "vs_baseline": value / (1.0 / PUBLISHED_GPU_S),
             "vs_baseline_source": "reference README.md:104-109 blend_big GPU PDHG 0.80 s at 1e-4 (unspecified GPU)",
             "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_DESC, "precision": "mixed (FP32 matrix+iterates, FP64 finish/certify)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "l2": "flushed (256 MiB write) before every timed step"},
+            "config": dict(CONFIG), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": "flushed (256 MiB write) before every timed step",
             "result": {"status": r_mixed.status_name, "iterations": r_mixed.iterations,
                        "fp32_iterations": r_mixed.fp32_iterations, "restarts": r_mixed.restarts,
                        "pobj": r_mixed.pobj, "rel_primal": r_mixed.rel_primal, "rel_dual": r_mixed.rel_dual,
@@ -776,6 +814,9 @@ def main():
                          "algorithmic_bytes_per_launch": dom[1], "launch_ms": dom[2],
                          "timing": f"{args.kernel_iters} back-to-back launches in a CUDA graph, CUDA events",
                          "kernel_choice": "the longer of the two iteration kernels in this timing",
+                         "working_set": "the FP32 iteration (64 MB) is L2-resident in the solve, so this fraction "
+                                        "of the HBM copy peak is reached on L2-served data; the HBM-bound "
+                                        "configuration is the 512-LP batch (batch.iteration_kernels)",
                          "kernels": pair},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "status": re2e.status_name, "setup_s_last": re2e.setup_seconds, "solve_s_last": re2e.solve_seconds,
@@ -788,6 +829,7 @@ def main():
             "diff": diff,
             "qp": qp,
             "strong_branching": branch,
+            "reference_cuda": refcuda,
         }
         print(json.dumps(line), flush=True)
     prob.close()

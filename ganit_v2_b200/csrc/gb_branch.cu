@@ -352,7 +352,10 @@ void strong_branch(const gb_lp& lp, const double* x, const double* y, int count,
         }
         const double cb = cert[c.inst];
         o.cert[d] = cb;
-        if (cb >= cutoff) o.z[d] = INFINITY;
+        // pruned when the certified bound reaches the cutoff, and -- as the
+        // reference's dual simplex returns Cutoff once its objective reaches
+        // it (src/mip.cpp:755) -- when a solved child's objective does
+        if (cb >= cutoff || (r.status == GB_OPTIMAL && r.pobj >= cutoff)) o.z[d] = INFINITY;
         else if (r.status == GB_OPTIMAL) o.z[d] = r.pobj;  // minimisation form (children are)
         else o.z[d] = std::isfinite(cb) ? std::max(node_obj, cb) : node_obj;
     }

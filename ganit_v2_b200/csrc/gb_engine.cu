@@ -251,6 +251,22 @@ __global__ void k_fill_segments(const int* off, int* out) {
 
 constexpr double kL2StreamBytes = 126.0e6;  // the B200's L2
 
+// Load mode of the iteration kernels forced by GANIT_B200_LOADS (plain,
+// stream or prefetch); -1 (unset or "auto"): chosen per matrix and precision
+// from the iteration's bytes against the L2.
+int load_mode_override() {
+    static const int mode = [] {
+        const char* v = std::getenv("GANIT_B200_LOADS");
+        if (v == nullptr) return -1;
+        const std::string s(v);
+        if (s == "plain") return static_cast<int>(kLoadPlain);
+        if (s == "stream") return static_cast<int>(kLoadStream);
+        if (s == "prefetch") return static_cast<int>(kLoadPrefetch);
+        return -1;
+    }();
+    return mode;
+}
+
 // Upload + device setup (scale_lp + estimate_norm + run_pdhg's start point)
 // of `count` instances.
 Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
@@ -458,7 +474,8 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     for (int w = 0; w < 2; ++w) {
         const double sm = w ? 8.0 : 4.0, sv = w ? 8.0 : 4.0;
         const double iter = 2.0 * static_cast<double>(P->A.nnz) * (sm + 4.0) + 4.0 * (m + n + 2) + sv * (9.0 * n + 7.0 * m);
-        const int nc = iter > kL2StreamBytes ? 1 : 0;
+        const int forced = load_mode_override();
+        const int nc = forced >= 0 ? forced : (iter > kL2StreamBytes ? kLoadStream : kLoadPlain);
         P->A.stream_nc[w] = P->AT.stream_nc[w] = nc;
     }
     if (P->has_q && !P->dplr) cvt32(P->Q);
@@ -594,6 +611,26 @@ void iteration_args(Problem& P, VecSet<V>& vs, int k, PrimalArgs<M, V>& pa, Dual
                         P.st.get()};
 }
 
+// The fused iteration kernels at their matrix view's load mode (CsrView::nc).
+template <class M, class V>
+void launch_primal(const PrimalArgs<M, V>& pa, cudaStream_t s) {
+    if (pa.AT.nc == kLoadPrefetch)
+        launch_pdl(k_primal<M, V, kLoadPrefetch>, pa.AT.nb, kThreads, spmv_smem_bytes<1, V>(), s, pa);
+    else if (pa.AT.nc == kLoadStream)
+        launch_pdl(k_primal<M, V, kLoadStream>, pa.AT.nb, kThreads, spmv_smem_bytes<1, V>(), s, pa);
+    else
+        launch_pdl(k_primal<M, V>, pa.AT.nb, kThreads, spmv_smem_bytes<1, V>(), s, pa);
+}
+template <class M, class V>
+void launch_dual(const DualArgs<M, V>& da, cudaStream_t s) {
+    if (da.A.nc == kLoadPrefetch)
+        launch_pdl(k_dual<M, V, kLoadPrefetch>, da.A.nb, kThreads, spmv_smem_bytes<1, V>(), s, da);
+    else if (da.A.nc == kLoadStream)
+        launch_pdl(k_dual<M, V, kLoadStream>, da.A.nb, kThreads, spmv_smem_bytes<1, V>(), s, da);
+    else
+        launch_pdl(k_dual<M, V>, da.A.nb, kThreads, spmv_smem_bytes<1, V>(), s, da);
+}
+
 // One PDHG iteration (k-th inside the body) on buffers selected by parity.
 template <class M, class V>
 void launch_iteration(Problem& P, VecSet<V>& vs, int k, cudaStream_t s, long long& nl, cudaEvent_t mid = nullptr) {
@@ -601,12 +638,9 @@ void launch_iteration(Problem& P, VecSet<V>& vs, int k, cudaStream_t s, long lon
     DualArgs<M, V> da;
     iteration_args<M, V>(P, vs, k, pa, da);
     if (P.has_q) launch_qx<M, V>(P, vs, pa.x, vs.qx.get(), s, nl);
-    constexpr size_t sm = spmv_smem_bytes<1, V>();
-    if (pa.AT.nc) launch_pdl(k_primal<M, V, true>, pa.AT.nb, kThreads, sm, s, pa);
-    else launch_pdl(k_primal<M, V>, pa.AT.nb, kThreads, sm, s, pa);
+    launch_primal<M, V>(pa, s);
     if (mid) GB_CUDA(cudaEventRecord(mid, s));
-    if (da.A.nc) launch_pdl(k_dual<M, V, true>, da.A.nb, kThreads, sm, s, da);
-    else launch_pdl(k_dual<M, V>, da.A.nb, kThreads, sm, s, da);
+    launch_dual<M, V>(da, s);
     nl += 2;
 }
 
@@ -1000,7 +1034,6 @@ void time_level_graph(Problem& P, int iters, double* msp, double* msd, double* m
     PrimalArgs<M, V> pa;
     DualArgs<M, V> da;
     iteration_args<M, V>(P, vs, 0, pa, da);
-    constexpr size_t sm = spmv_smem_bytes<1, V>();
     auto timed_graph = [&](auto&& body) {
         cudaStream_t cs;
         GB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
@@ -1035,16 +1068,10 @@ void time_level_graph(Problem& P, int iters, double* msp, double* msd, double* m
         return static_cast<double>(ms) / iters;
     };
     *msp = timed_graph([&](cudaStream_t cs) {
-        for (int k = 0; k < iters; ++k) {
-            if (pa.AT.nc) launch_pdl(k_primal<M, V, true>, pa.AT.nb, kThreads, sm, cs, pa);
-            else launch_pdl(k_primal<M, V>, pa.AT.nb, kThreads, sm, cs, pa);
-        }
+        for (int k = 0; k < iters; ++k) launch_primal<M, V>(pa, cs);
     });
     *msd = timed_graph([&](cudaStream_t cs) {
-        for (int k = 0; k < iters; ++k) {
-            if (da.A.nc) launch_pdl(k_dual<M, V, true>, da.A.nb, kThreads, sm, cs, da);
-            else launch_pdl(k_dual<M, V>, da.A.nb, kThreads, sm, cs, da);
-        }
+        for (int k = 0; k < iters; ++k) launch_dual<M, V>(da, cs);
     });
     *msi = timed_graph([&](cudaStream_t cs) {
         long long nl = 0;

@@ -76,6 +76,14 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
+// "Active" flag of an instance read before the programmatic-launch wait (a
+// prefetching kernel's hint): possibly stale, but inside a phase the flag only
+// goes from 1 to 0 (k_decide clears it; it is set only by the phase set-up
+// before the phase's graph starts), so a stale value only errs towards true.
+__device__ __forceinline__ bool active_hint(const SolveState* st, int inst) {
+    return *reinterpret_cast<const volatile int*>(&st[inst].active) != 0;
+}
+
 // ---------------------------------------------------------------- iteration kernels
 // Minimum resident CTAs per SM requested from the register allocator.
 template <class V>
@@ -105,6 +113,16 @@ struct PrimalEpi {
         tau = static_cast<V>(s.tau);
         return s.active != 0;
     }
+    __device__ __forceinline__ bool hint(int inst) const { return active_hint(a->st, inst); }
+    __device__ __forceinline__ void l2_prefetch_rows(int r0, int r1) const {
+        const size_t k = sizeof(V) * static_cast<size_t>(r1 - r0);
+        l2_prefetch(a->x + r0, k);
+        l2_prefetch(a->c + r0, k);
+        l2_prefetch(a->l + r0, k);
+        l2_prefetch(a->u + r0, k);
+        l2_prefetch(a->sumx + r0, k);
+        if (a->qx) l2_prefetch(a->qx + r0, k);
+    }
     struct Pre {
         V x, c, l, u, sumx, qx;
     };
@@ -122,12 +140,16 @@ struct PrimalEpi {
     }
 };
 
-template <class M, class V, bool NC = false>
+template <class M, class V, int L = kLoadPlain>
 __global__ void __launch_bounds__(kThreads, kMinCtas<V>) k_primal(const __grid_constant__ PrimalArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    pdl_enter();
     PrimalEpi<M, V> epi{&a, V(0)};
-    spmv_run<1, M, V, NC>(a.AT, blockIdx.x, GatherOne<V>{a.y}, epi, smem);
+    if constexpr (L == kLoadPrefetch) {
+        spmv_run_prefetched<1, M, V>(a.AT, blockIdx.x, GatherOne<V>{a.y}, epi, smem);
+    } else {
+        pdl_enter();
+        spmv_run<1, M, V, L == kLoadStream>(a.AT, blockIdx.x, GatherOne<V>{a.y}, epi, smem);
+    }
 }
 
 template <class M, class V>
@@ -151,6 +173,14 @@ struct DualEpi {
         sigma = static_cast<V>(s.sigma);
         return s.active != 0;
     }
+    __device__ __forceinline__ bool hint(int inst) const { return active_hint(a->st, inst); }
+    __device__ __forceinline__ void l2_prefetch_rows(int r0, int r1) const {
+        const size_t k = sizeof(V) * static_cast<size_t>(r1 - r0);
+        l2_prefetch(a->y + r0, k);
+        l2_prefetch(a->lo + r0, k);
+        l2_prefetch(a->hi + r0, k);
+        l2_prefetch(a->sumy + r0, k);
+    }
     struct Pre {
         V y, lo, hi, sumy;
     };
@@ -167,12 +197,16 @@ struct DualEpi {
     }
 };
 
-template <class M, class V, bool NC = false>
+template <class M, class V, int L = kLoadPlain>
 __global__ void __launch_bounds__(kThreads, kMinCtas<V>) k_dual(const __grid_constant__ DualArgs<M, V> a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    pdl_enter();
     DualEpi<M, V> epi{&a, V(0)};
-    spmv_run<1, M, V, NC>(a.A, blockIdx.x, GatherOne<V>{a.xbar}, epi, smem);
+    if constexpr (L == kLoadPrefetch) {
+        spmv_run_prefetched<1, M, V>(a.A, blockIdx.x, GatherOne<V>{a.xbar}, epi, smem);
+    } else {
+        pdl_enter();
+        spmv_run<1, M, V, L == kLoadStream>(a.A, blockIdx.x, GatherOne<V>{a.xbar}, epi, smem);
+    }
 }
 
 // ---------------------------------------------------------------- KKT evaluation

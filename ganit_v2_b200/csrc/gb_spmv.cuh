@@ -205,17 +205,19 @@ struct CsrView {
     // nonzero (allocated with padded_nnz), so STREAM blocks use 16-byte loads.
     // Views of caller-owned arrays leave it 0 (scalar loads).
     int vec = 0;
-    // 1: launch the iteration kernels' variant whose 16-byte idx / val loads
-    // skip L1 allocation (spmv_run<..., true>: ld.global.nc with
-    // L1::no_allocate), set when an iteration's data at this precision does
-    // not fit in L2 and so streams from HBM.  Measured on B200: -15% per
-    // iteration on the 512-LP batch (207 MB per FP32 iteration), neutral to
-    // +8% per kernel on the blending LP at FP64 (104 MB), +20% on it at FP32
-    // (64 MB, L2-resident); so only iterations above the L2 size switch.  A
-    // template choice, not a branch: a branch in the loop costs the
-    // 32-register kernels spills.
+    // Load mode of the iteration kernels (LoadMode; a template choice, not a
+    // branch: a branch in the loop costs the 32-register kernels spills).
+    // kLoadStream: the 16-byte idx / val loads skip L1 allocation
+    // (ld.global.nc with L1::no_allocate), for iterations whose data at this
+    // precision does not fit in L2 and so streams from HBM.  Measured on
+    // B200: -15% per iteration on the 512-LP batch (207 MB per FP32
+    // iteration), neutral to +8% per kernel on the blending LP at FP64
+    // (104 MB), +20% on it at FP32 (64 MB, L2-resident).  kLoadPrefetch: the
+    // same loads after bulk L2 prefetches (spmv_run_prefetched).
     int nc = 0;
 };
+
+enum LoadMode : int { kLoadPlain = 0, kLoadStream = 1, kLoadPrefetch = 2 };
 
 // Element count of idx / val arrays allocated for 16-byte loads (CsrView::vec).
 inline long long padded_nnz(long long nnz) { return ((nnz + 3) & ~3LL) + 4; }
@@ -256,6 +258,20 @@ __device__ __forceinline__ void load4_stream(const double* p, double (&o)[4]) {
 }
 __device__ __forceinline__ void load4_stream(const __nv_bfloat16* p, __nv_bfloat16 (&o)[4]) { load4(p, o); }
 
+// Bulk prefetch of [p, p + bytes) into L2 (cp.async.bulk.prefetch.L2,
+// sm_90+): one instruction, no shared memory, no registers held and nothing
+// to wait for -- a hint that starts the DRAM reads early.  The range is cut
+// to the whole 16-byte units inside it (the instruction wants a 16-byte
+// aligned start and a size in 16-byte units), so no byte outside
+// [p, p + bytes) is touched.
+__device__ __forceinline__ void l2_prefetch(const void* p, size_t bytes) {
+    const unsigned long long a = reinterpret_cast<unsigned long long>(p);
+    const unsigned long long s = (a + 15ull) & ~15ull, e = (a + bytes) & ~15ull;
+    if (e > s)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(s), "r"(static_cast<unsigned>(e - s))
+                     : "memory");
+}
+
 // Gather of a single right-hand side.
 template <class V>
 struct GatherOne {
@@ -277,6 +293,7 @@ template <int NV, class V>
 constexpr size_t spmv_smem_bytes() {
     return sizeof(V) * NV * kProdStride + sizeof(double) * kWarps * NV + 64;
 }
+
 
 // LONG / CHUNK block: whole CTA strides over the slice, block reduction,
 // epilogue by thread 0 (CHUNK: the last CTA to arrive).  `red` holds
@@ -427,6 +444,35 @@ __device__ __forceinline__ void spmv_run(const CsrView<M>& A, int cta, const Gat
     }
     __syncthreads();
     reduce_rows<NV, V>(b, prod, s, e, act, pre, epi);
+}
+
+// Load mode kLoadPrefetch of the iteration kernels (which must NOT call
+// pdl_enter themselves): the schedule and the matrix are written once at
+// set-up, so before the programmatic-launch wait one thread reads the CTA's
+// block and asks L2 for its whole idx / val window and for the rows'
+// epilogue operands (epi.l2_prefetch_rows) with bulk prefetches.  The DRAM
+// reads then overlap the previous kernel's last wave and this CTA's own
+// dependent start-up loads, and the loop's 16-byte loads find the data in
+// L2 -- without the shared memory a staging copy would take from the L1
+// carve-out the gathers hit.  L2 is the coherence point of device memory, so
+// prefetching vectors that the previous kernel may still be writing is only
+// a hint, never a stale read.  epi.hint(inst) may read stale per-instance
+// state (it runs before the wait) and must only err towards true.  Results
+// are bit-identical to spmv_run.
+template <int NV, class M, class V, class Gather, class Epi>
+__device__ __forceinline__ void spmv_run_prefetched(const CsrView<M>& A, int cta, const Gather& g, Epi& epi,
+                                                    unsigned char* smem) {
+    if (threadIdx.x == 0) {
+        const RowBlock b = A.blocks[cta];
+        if (epi.hint(b.inst)) {
+            const size_t cnt = static_cast<size_t>(b.p1 - b.p0);
+            l2_prefetch(A.idx + b.p0, sizeof(int) * cnt);
+            l2_prefetch(A.val + b.p0, sizeof(M) * cnt);
+            epi.l2_prefetch_rows(b.r0, b.r1);
+        }
+    }
+    pdl_enter();
+    spmv_run<NV, M, V, true>(A, cta, g, epi, smem);
 }
 
 }  // namespace gb

@@ -376,9 +376,16 @@ void gb_factor_free(gb_factor* f);
  * Objectives are in minimisation form (a maximisation LP's are negated), and
  * node_obj / cutoff are too (cutoff = INFINITY: no incumbent).
  * Per child (index 0 = down, 1 = up), as src/mip.cpp:750-763: z = +INF when
- * the child is primal infeasible (also when its bounds cross) or its
- * certified bound is >= cutoff; else its objective when GB_OPTIMAL; else
- * max(node_obj, cert), or node_obj when cert = -INF (not certifiable). */
+ * the child is primal infeasible (also when its bounds cross), when its
+ * certified bound is >= cutoff, or when it is GB_OPTIMAL with an objective
+ * >= cutoff (the reference's dual simplex stops with Cutoff there); else its
+ * objective when GB_OPTIMAL; else max(node_obj, cert), or node_obj when
+ * cert = -INF (not certifiable).
+ * The certified bound uses the child's own column bounds: unlike
+ * Mip::safe_bound (src/mip.cpp:361-364), no implied bounds replace infinite
+ * ones, so a child with an unbounded column whose reduced-cost interval has
+ * the wrong sign gets cert = -INF where the reference may certify a finite
+ * bound. */
 typedef struct {
     double z[2];          /* child objective estimate */
     double cert[2];       /* certified lower bound (+INF: infeasible; -INF: none) */

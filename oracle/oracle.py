@@ -90,6 +90,7 @@ def build(ref: bool = True) -> None:
         lib = os.path.join(os.path.dirname(HERE), "ganit_v2_b200", "libganit_b200.so")
         if os.path.exists(lib):
             targets.append("dropin")
+        targets.append("refcuda")
     subprocess.run(["make", "-s", "-C", HERE, f"REF={REF_ROOT}"] + targets, check=True)
 
 
@@ -226,6 +227,35 @@ def ref_solve(lp, threads: int | None = None, **opts) -> OracleResult:
            C.byref(o), C.byref(r), _p(x), _p(y))
     if rc != 0:
         raise RuntimeError("reference solve_pdhg_cpu threw")
+    return OracleResult(STATUS[r.status], r.pobj, r.dobj, r.rel_p, r.rel_d, r.rel_gap, r.iterations,
+                        r.fp32_iterations, r.l2_iterations, r.restarts, r.setup_s, r.solve_s, x, y)
+
+
+REFCUDA_SO = os.path.join(HERE, "_ref", "libganit_refcuda.so")
+
+
+def refcuda_available() -> bool:
+    return os.path.exists(REFCUDA_SO)
+
+
+def refcuda_solve(lp, **opts) -> OracleResult:
+    """Run the UNMODIFIED reference ganit::solve_pdhg_gpu (src/backend_cuda.cu,
+    built for sm_100a; needs a GPU).  LPs only."""
+    lib = _load(REFCUDA_SO)
+    a = _arrays(lp)
+    if a["qptr"] is not None:
+        raise ValueError("refcuda_solve takes LPs only")
+    o = _options(**opts)
+    r = _RefRes()
+    x = np.zeros(lp.n)
+    y = np.zeros(lp.m)
+    f = lib.refcuda_solve_pdhg_gpu
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 8 + [C.c_double, C.c_int] + [C.c_void_p] * 4
+    rc = f(lp.m, lp.n, _p(a["ptr"]), _p(a["idx"]), _p(a["val"]), _p(a["c"]), _p(a["l"]), _p(a["u"]), _p(a["lo"]),
+           _p(a["hi"]), float(lp.obj_const), int(lp.maximize), C.byref(o), C.byref(r), _p(x), _p(y))
+    if rc != 0:
+        raise RuntimeError("reference solve_pdhg_gpu threw")
     return OracleResult(STATUS[r.status], r.pobj, r.dobj, r.rel_p, r.rel_d, r.rel_gap, r.iterations,
                         r.fp32_iterations, r.l2_iterations, r.restarts, r.setup_s, r.solve_s, x, y)
 

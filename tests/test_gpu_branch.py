@@ -148,19 +148,31 @@ def test_crossing_bounds_need_no_solve(gb, node, opt):
         assert (sb.action, sb.lo, sb.hi) == (gb.BRANCH_TIGHTEN, np.ceil(x[j]), lp.u[j])
 
 
-def test_cutoff_prunes_on_certified_bounds_only(gb, oracle_built, node, opt):
+def test_cutoff_prunes_like_the_reference(gb, oracle_built, node, opt):
+    """A finite cutoff between the children's optima: a child is pruned
+    (z = +inf) exactly where the reference's rule prunes it -- its optimum
+    reaches the cutoff (the dual simplex returns Cutoff, src/mip.cpp:755) --
+    and the decision is the oracle's."""
     lp, x, z = node
-    cands = gb.most_fractional(x, [j for j in gb.fractional(x, lp.is_int) if j < 120], 4)
-    free = gb.strong_branch(lp, x, cands, z, opt=opt)
-    finite = free.cert[np.isfinite(free.cert)]
-    cutoff = float(np.median(finite))
+    planted = set(np.concatenate([lp.meta["up_blocked"], lp.meta["down_blocked"], lp.meta["both_blocked"]]))
+    cands = gb.most_fractional(x, [j for j in gb.fractional(x, lp.is_int) if j not in planted], 6)
+    free = oracle_built.strong_branch_reference(lp, x, cands, z)
+    finite = np.sort(free["z"][np.isfinite(free["z"])])
+    # a cutoff halfway between two distinct optima, so no child sits within the tolerance of it
+    gaps = np.diff(finite)
+    i = int(np.argmax(gaps[len(gaps) // 4:])) + len(gaps) // 4
+    cutoff = float(0.5 * (finite[i] + finite[i + 1]))
+    assert gaps[i] > 1e-4 * (1 + abs(cutoff))
+    ref = oracle_built.strong_branch_reference(lp, x, cands, z, cutoff=cutoff)
     cut = gb.strong_branch(lp, x, cands, z, cutoff=cutoff, opt=opt)
-    for t in range(len(cands)):
-        for d in range(2):
-            if free.cert[t, d] >= cutoff:
-                assert np.isinf(cut.z[t, d])
-            else:
-                assert cut.z[t, d] == free.z[t, d]
+    pruned = np.isinf(ref["z"]) & np.isfinite(free["z"])
+    assert pruned.any()
+    np.testing.assert_array_equal(np.isinf(cut.z), np.isinf(ref["z"]))
+    fin = np.isfinite(ref["z"])
+    np.testing.assert_allclose(cut.z[fin], ref["z"][fin], rtol=1e-5, atol=1e-5)
+    assert cut.action == ref["action"]
+    if ref["action"] != gb.BRANCH_VAR:
+        assert cut.var == ref["var"]
 
 
 def test_maximisation_is_branched_in_minimisation_form(gb, oracle_built, node, opt):

