@@ -154,7 +154,8 @@ class _GbDiffInfo(C.Structure):
     _fields_ = [("tau", C.c_double), ("sigma", C.c_double), ("tail_iterations", C.c_int64),
                 ("checkpoint_every", C.c_int64), ("implicit_iterations", C.c_int64), ("implicit_residual", C.c_double),
                 ("implicit_converged", C.c_int32), ("free_cols", C.c_int32), ("active_rows", C.c_int32),
-                ("polished", C.c_int32), ("polish_iterations", C.c_int64), ("launches", C.c_int64)]
+                ("polished", C.c_int32), ("active_set_repaired", C.c_int32), ("pad", C.c_int32),
+                ("polish_iterations", C.c_int64), ("launches", C.c_int64)]
 
 
 class GbKkt(C.Structure):

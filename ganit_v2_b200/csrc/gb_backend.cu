@@ -202,6 +202,7 @@ CsrView<M> bview(const DevBuf<int>& ptr, const DevBuf<int>& idx, const DevBuf<un
     v.blocks = s.blocks.get();
     v.slots = s.slots.get();
     v.counters = s.counters.get();
+    v.bits = s.bits.get();
     v.rows = rows;
     v.nb = s.nb;
     return v;

@@ -230,11 +230,14 @@ struct MrVecs {
 };
 
 // Right-hand side (mu_x on free columns; mu_y on dual-active rows), v_1 = b / beta_1.
+// Instances with sel[k] == 0 (sel != nullptr) keep their state and solution.
 __global__ void __launch_bounds__(kThreads) k_mr_init(const __grid_constant__ MrVecs a, const double* __restrict__ mux,
-                                                      const double* __restrict__ muy, long long max_it, double tol) {
+                                                      const double* __restrict__ muy, long long max_it, double tol,
+                                                      const int* __restrict__ sel) {
     __shared__ double red[kWarps * 3];
     __shared__ double inv;
     const int k = blockIdx.x;
+    if (sel != nullptr && sel[k] == 0) return;
     const int c0 = a.col_off[k], c1 = a.col_off[k + 1], r0 = a.row_off[k], r1 = a.row_off[k + 1];
     double v[3] = {0.0, 0.0, 0.0};
     for (int j = c0 + threadIdx.x; j < c1; j += kThreads) {
@@ -580,12 +583,14 @@ struct Diff {
     // Per-instance MINRES on K = [[0, B^T], [B, 0]] with B = A'[D, F] read from
     // the codes of step 0 of the resident segment; solution in mr[10], mr[11];
     // per-instance state left in mst_host.
-    void minres(const double* rhs_x, const double* rhs_y) {
+    // sel (device, may be NULL): only the instances with sel[k] != 0 start a
+    // new solve; the others keep their state and solution.
+    void minres(const double* rhs_x, const double* rhs_y, const int* sel = nullptr) {
         Problem& p = *P;
         cudaStream_t s = p.stream;
         const size_t smem = spmv_smem_bytes<1, double>();
         MrVecs v = mr_vecs();
-        k_mr_init<<<p.count, kThreads, 0, s>>>(v, rhs_x, rhs_y, mr_max, mr_tol);
+        k_mr_init<<<p.count, kThreads, 0, s>>>(v, rhs_x, rhs_y, mr_max, mr_tol, sel);
         launches += 1;
         MrOpArgs oa{p.A.view<double>(), p.AT.view<double>(), v};
         const int nb = oa.A.nb + oa.AT.nb;
@@ -637,6 +642,75 @@ inline double kkt_err(const Kkt& k) {
     return std::isfinite(e) ? e : INFINITY;
 }
 
+// Active-set repair after a first polishing solve.  An instance whose reduced
+// system did not converge and whose active set is not square (|D| dual-active
+// rows != |F| free columns; a nondegenerate vertex has a square, nonsingular
+// basis B = A'[D, F]) was read off a point whose smallest duals or slacks are
+// within the solve tolerance of zero, so one PDHG step classified them
+// wrongly.  Its excess rows (|D| > |F|) leave D smallest |y+| first (equality
+// rows never leave); its excess columns (|F| > |D|) go to their nearest finite
+// bound, nearest first.  The codes are changed in place (they define the
+// reduced system and the polished point) and D.flags selects the repaired
+// instances.  Returns whether any instance was repaired.
+bool repair_active_sets(Diff& D) {
+    Problem& P = *D.P;
+    cudaStream_t s = P.stream;
+    std::vector<int> fix;
+    for (int k = 0; k < P.count; ++k) {
+        const MrState& st = D.mst_host[k];
+        if (!st.converged && st.free_cols != st.active_rows) fix.push_back(k);
+    }
+    if (fix.empty()) return false;
+    const size_t n = D.n(), m = D.m();
+    std::vector<i8> cx(n), cy(m);
+    std::vector<double> x1(n), y1(m), l(n), u(n), lo(m), hi(m);
+    GB_CUDA(cudaMemcpyAsync(cx.data(), D.cx_at(0), n, cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaMemcpyAsync(cy.data(), D.cy_at(0), m, cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaMemcpyAsync(x1.data(), D.x_at(1), n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaMemcpyAsync(y1.data(), D.y_at(1), m * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaMemcpyAsync(l.data(), P.l.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaMemcpyAsync(u.data(), P.u.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaMemcpyAsync(lo.data(), P.lo.get(), m * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaMemcpyAsync(hi.data(), P.hi.get(), m * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < P.count; ++k) D.flags_host[k] = 0;
+    bool any = false;
+    for (int k : fix) {
+        const int c0 = P.col_off[k], c1 = P.col_off[k + 1], r0 = P.row_off[k], r1 = P.row_off[k + 1];
+        std::vector<std::pair<double, int>> cand;
+        const int excess = D.mst_host[k].active_rows - D.mst_host[k].free_cols;
+        if (excess > 0) {
+            for (int i = r0; i < r1; ++i)
+                if (cy[i] != 0 && lo[i] < hi[i]) cand.push_back({std::fabs(y1[i]), i});
+        } else {
+            for (int j = c0; j < c1; ++j) {
+                if (cx[j] != 1) continue;
+                double d = INFINITY;
+                if (std::isfinite(l[j])) d = std::min(d, x1[j] - l[j]);
+                if (std::isfinite(u[j])) d = std::min(d, u[j] - x1[j]);
+                if (std::isfinite(d)) cand.push_back({d, j});
+            }
+        }
+        const int need = std::abs(excess);
+        if (static_cast<int>(cand.size()) < need) continue;
+        std::partial_sort(cand.begin(), cand.begin() + need, cand.end());
+        for (int t = 0; t < need; ++t) {
+            const int e = cand[t].second;
+            if (excess > 0) cy[e] = 0;
+            else cx[e] = (std::isfinite(l[e]) && (!std::isfinite(u[e]) || x1[e] - l[e] <= u[e] - x1[e])) ? 0 : 2;
+        }
+        D.flags_host[k] = 1;
+        D.info[k].active_set_repaired = 1;
+        any = true;
+    }
+    if (!any) return false;
+    GB_CUDA(cudaMemcpyAsync(D.cx_at(0), cx.data(), n, cudaMemcpyHostToDevice, s));
+    GB_CUDA(cudaMemcpyAsync(D.cy_at(0), cy.data(), m, cudaMemcpyHostToDevice, s));
+    D.flags.upload(D.flags_host, P.count, s);
+    GB_CUDA(cudaStreamSynchronize(s));  // the host vectors above go out of scope
+    return true;
+}
+
 // Polishing (the reduced KKT solve of OSQP-style solvers): per instance,
 // replace the PDHG point by the vertex of the active set one PDHG step reads
 // off it, when that vertex certifies better in FP64.
@@ -663,6 +737,15 @@ void polish(Diff& D) {
     }
     D.launches += 2;
     D.minres(rhs_x, rhs_y);
+    if (repair_active_sets(D)) {  // second solve on the instances whose active set was repaired
+        k_polish_rhs_cols<<<gv, kThreads, 0, s>>>(n, D.cx_at(0), P.c.get(), P.l.get(), P.u.get(), rhs_x, xn);
+        if (P.A.sched.nb) {
+            PolishRowEpi e{D.cy_at(0), P.lo.get(), P.hi.get(), rhs_y};
+            k_polish_rhs_rows<<<P.A.sched.nb, kThreads, spmv_smem_bytes<1, double>(), s>>>(P.A.view<double>(), xn, e);
+        }
+        D.launches += 2;
+        D.minres(rhs_x, rhs_y, D.flags.get());
+    }
     for (int k = 0; k < P.count; ++k) {
         D.flags_host[k] = D.mst_host[k].converged ? 1 : 0;
         D.info[k].polish_iterations = D.mst_host[k].it;
@@ -827,6 +910,17 @@ void diff_backward(Diff& D, const double* dl_dx, const double* dl_dy, double* dl
                                           P.C.get(), P.R.get(), D.gc.get(), D.glo.get(), D.ghi.get(), D.ga.get(),
                                           D.io_n.get(), D.io_m.get(), D.io_m2.get(), D.io_z.get());
     D.launches += 1;
+    // an instance whose completion did not converge gets NaN gradients (all bytes 0xff), not unverified values
+    if (D.mr_max > 0)
+        for (int k = 0; k < P.count; ++k) {
+            if (D.mst_host[k].converged) continue;
+            const size_t c0 = P.col_off[k], c1 = P.col_off[k + 1], r0 = P.row_off[k], r1 = P.row_off[k + 1];
+            const size_t z0 = P.nnz_off[k], z1 = P.nnz_off[k + 1];
+            GB_CUDA(cudaMemsetAsync(D.io_n.get() + c0, 0xff, (c1 - c0) * sizeof(double), s));
+            GB_CUDA(cudaMemsetAsync(D.io_m.get() + r0, 0xff, (r1 - r0) * sizeof(double), s));
+            GB_CUDA(cudaMemsetAsync(D.io_m2.get() + r0, 0xff, (r1 - r0) * sizeof(double), s));
+            if (z1 > z0) GB_CUDA(cudaMemsetAsync(D.io_z.get() + z0, 0xff, (z1 - z0) * sizeof(double), s));
+        }
     if (dl_dc) GB_CUDA(cudaMemcpyAsync(dl_dc, D.io_n.get(), nb, cudaMemcpyDeviceToHost, s));
     if (dl_dlo) GB_CUDA(cudaMemcpyAsync(dl_dlo, D.io_m.get(), mb, cudaMemcpyDeviceToHost, s));
     if (dl_dhi) GB_CUDA(cudaMemcpyAsync(dl_dhi, D.io_m2.get(), mb, cudaMemcpyDeviceToHost, s));

@@ -615,20 +615,20 @@ void iteration_args(Problem& P, VecSet<V>& vs, int k, PrimalArgs<M, V>& pa, Dual
 template <class M, class V>
 void launch_primal(const PrimalArgs<M, V>& pa, cudaStream_t s) {
     if (pa.AT.nc == kLoadPrefetch)
-        launch_pdl(k_primal<M, V, kLoadPrefetch>, pa.AT.nb, kThreads, spmv_smem_bytes<1, V>(), s, pa);
+        launch_pdl(k_primal<M, V, kLoadPrefetch>, pa.AT.nb, kThreads, spmv_seg_smem_bytes<V>(), s, pa);
     else if (pa.AT.nc == kLoadStream)
-        launch_pdl(k_primal<M, V, kLoadStream>, pa.AT.nb, kThreads, spmv_smem_bytes<1, V>(), s, pa);
+        launch_pdl(k_primal<M, V, kLoadStream>, pa.AT.nb, kThreads, spmv_seg_smem_bytes<V>(), s, pa);
     else
-        launch_pdl(k_primal<M, V>, pa.AT.nb, kThreads, spmv_smem_bytes<1, V>(), s, pa);
+        launch_pdl(k_primal<M, V>, pa.AT.nb, kThreads, spmv_seg_smem_bytes<V>(), s, pa);
 }
 template <class M, class V>
 void launch_dual(const DualArgs<M, V>& da, cudaStream_t s) {
     if (da.A.nc == kLoadPrefetch)
-        launch_pdl(k_dual<M, V, kLoadPrefetch>, da.A.nb, kThreads, spmv_smem_bytes<1, V>(), s, da);
+        launch_pdl(k_dual<M, V, kLoadPrefetch>, da.A.nb, kThreads, spmv_seg_smem_bytes<V>(), s, da);
     else if (da.A.nc == kLoadStream)
-        launch_pdl(k_dual<M, V, kLoadStream>, da.A.nb, kThreads, spmv_smem_bytes<1, V>(), s, da);
+        launch_pdl(k_dual<M, V, kLoadStream>, da.A.nb, kThreads, spmv_seg_smem_bytes<V>(), s, da);
     else
-        launch_pdl(k_dual<M, V>, da.A.nb, kThreads, spmv_smem_bytes<1, V>(), s, da);
+        launch_pdl(k_dual<M, V>, da.A.nb, kThreads, spmv_seg_smem_bytes<V>(), s, da);
 }
 
 // One PDHG iteration (k-th inside the body) on buffers selected by parity.

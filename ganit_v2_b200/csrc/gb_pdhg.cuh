@@ -145,10 +145,10 @@ __global__ void __launch_bounds__(kThreads, kMinCtas<V>) k_primal(const __grid_c
     extern __shared__ __align__(16) unsigned char smem[];
     PrimalEpi<M, V> epi{&a, V(0)};
     if constexpr (L == kLoadPrefetch) {
-        spmv_run_prefetched<1, M, V>(a.AT, blockIdx.x, GatherOne<V>{a.y}, epi, smem);
+        spmv_run_prefetched<M, V>(a.AT, blockIdx.x, GatherOne<V>{a.y}, epi, smem);
     } else {
         pdl_enter();
-        spmv_run<1, M, V, L == kLoadStream>(a.AT, blockIdx.x, GatherOne<V>{a.y}, epi, smem);
+        spmv_run_iter<M, V, L == kLoadStream>(a.AT, blockIdx.x, GatherOne<V>{a.y}, epi, smem);
     }
 }
 
@@ -202,10 +202,10 @@ __global__ void __launch_bounds__(kThreads, kMinCtas<V>) k_dual(const __grid_con
     extern __shared__ __align__(16) unsigned char smem[];
     DualEpi<M, V> epi{&a, V(0)};
     if constexpr (L == kLoadPrefetch) {
-        spmv_run_prefetched<1, M, V>(a.A, blockIdx.x, GatherOne<V>{a.xbar}, epi, smem);
+        spmv_run_prefetched<M, V>(a.A, blockIdx.x, GatherOne<V>{a.xbar}, epi, smem);
     } else {
         pdl_enter();
-        spmv_run<1, M, V, L == kLoadStream>(a.A, blockIdx.x, GatherOne<V>{a.xbar}, epi, smem);
+        spmv_run_iter<M, V, L == kLoadStream>(a.A, blockIdx.x, GatherOne<V>{a.xbar}, epi, smem);
     }
 }
 

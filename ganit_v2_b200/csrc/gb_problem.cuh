@@ -40,6 +40,7 @@ struct DevMat {
         v.blocks = sc.blocks.get();
         v.slots = sc.slots.get();
         v.counters = sc.counters.get();
+        v.bits = sc.bits.get();
         v.rows = rows;
         v.nb = sc.nb;
         v.vec = 1;  // upload_mat / device_transpose / cvt32 allocate padded_nnz, cudaMalloc aligns

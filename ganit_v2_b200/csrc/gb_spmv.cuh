@@ -61,7 +61,26 @@ struct Schedule {
     std::vector<int> seg_block;
     int nslots = 0, ncounters = 0;
     int max_lg = 0;
+    // Row-start bitmaps of the STREAM blocks (the iteration kernels' segmented
+    // reduction, spmv_run_seg): block b's words start at b.slot_base; bit t of
+    // its window (t = element - 4 floor(p0 / 4)) is set where a non-empty row
+    // begins.
+    std::vector<unsigned> bits;
 };
+
+// Appends the row-start bitmap of a STREAM block to s.bits and records its
+// offset in b.slot_base (a field CHUNK blocks use for their slots).
+inline void add_stream_bits(Schedule& s, const int* ptr, RowBlock& b) {
+    const int a = b.p0 & 3, nq = ((b.p1 + 3) >> 2) - (b.p0 >> 2);
+    const size_t off = s.bits.size();
+    s.bits.resize(off + (4 * static_cast<size_t>(nq) + 31) / 32, 0u);
+    for (int i = b.r0; i < b.r1; ++i)
+        if (ptr[i + 1] > ptr[i]) {
+            const int t = ptr[i] - b.p0 + a;
+            s.bits[off + (t >> 5)] |= 1u << (t & 31);
+        }
+    b.slot_base = static_cast<int>(off);
+}
 
 inline int floor_log2(int v) {
     int l = 0;
@@ -143,6 +162,7 @@ inline Schedule build_schedule(const int* ptr, int rows, const int* seg_off = nu
         const int r0 = seg_off ? seg_off[k] : 0, r1 = seg_off ? seg_off[k + 1] : rows;
         schedule_rows(ptr, r0, r1, block_nnz, max_rows, &s.nslots, &s.ncounters, k, [&](const RowBlock& b) {
             s.blocks.push_back(b);
+            if (b.kind == kStream) add_stream_bits(s, ptr, s.blocks.back());
             s.max_lg = std::max(s.max_lg, b.lg);
         });
     }
@@ -160,6 +180,7 @@ inline Schedule build_schedule(const int* ptr, const int* seg_off, int nseg, con
         schedule_rows(ptr, seg_off[k], seg_off[k + 1], block_nnz[k], max_rows[k], &s.nslots, &s.ncounters, k,
                       [&](const RowBlock& b) {
                           s.blocks.push_back(b);
+                          if (b.kind == kStream) add_stream_bits(s, ptr, s.blocks.back());
                           s.max_lg = std::max(s.max_lg, b.lg);
                       });
     }
@@ -173,6 +194,7 @@ struct DevSchedule {
     DevBuf<int> seg_block;  // per-instance block ranges
     DevBuf<double> slots;
     DevBuf<unsigned> counters;
+    DevBuf<unsigned> bits;  // Schedule::bits
     int nb = 0;
     int nslots = 0;
     std::vector<int> host_seg_block;
@@ -187,6 +209,8 @@ struct DevSchedule {
         slots.reset(static_cast<size_t>(s.nslots ? s.nslots : 1) * nv_max);
         counters.reset(s.ncounters ? s.ncounters : 1);
         GB_CUDA(cudaMemsetAsync(counters.get(), 0, counters.size() * sizeof(unsigned), st));
+        bits.reset(s.bits.empty() ? 1 : s.bits.size());
+        bits.upload(s.bits.data(), s.bits.size(), st);
     }
 };
 
@@ -199,6 +223,7 @@ struct CsrView {
     const RowBlock* __restrict__ blocks;
     double* slots;
     unsigned* counters;
+    const unsigned* __restrict__ bits;  // row-start bitmaps of the STREAM blocks (Schedule::bits), or nullptr
     int rows;
     int nb;
     // 1: idx / val are 16-byte aligned and readable 3 elements past the last
@@ -446,6 +471,157 @@ __device__ __forceinline__ void spmv_run(const CsrView<M>& A, int cta, const Gat
     reduce_rows<NV, V>(b, prod, s, e, act, pre, epi);
 }
 
+// ---------------------------------------------------------------- warp-segmented STREAM blocks
+// The FP64 iteration kernels' STREAM blocks (one right-hand side) reduce their
+// rows in registers instead of staging every product in shared memory (see
+// spmv_run_iter for the measured choice).  Measured on B200 (ncu, 512-LP
+// batch), the staged form spends ~1/3 of the L1TEX data-pipe wavefronts -- the
+// unit that bounds these kernels -- on the product stores and on row
+// reductions whose rows start at random banks.  Here:
+//   * a bitmap over the block's 4-aligned window (positions 0 .. 4 nq - 1),
+//     built with the schedule (Schedule::bits), marks each non-empty row's
+//     first element;
+//   * warp w takes chunks c = w, w + 8, ... of 32 quads (128 positions); each
+//     lane forms its quad's products and a segmented prefix within the quad,
+//     and the warp a segmented inclusive scan of the lanes' open parts (the
+//     head of a lane is its last row start, found with a ballot), so every
+//     element knows the sum of its row from the row's start, or from the
+//     chunk's start if the row began earlier, up to itself;
+//   * an element that ends its row's part of the chunk (the next element
+//     starts a row, the row ends, or the chunk ends) stores that sum at its
+//     own position;
+//   * thread i then adds, for row i, the parts stored at the ends of its
+//     pieces in each chunk it reaches, in chunk order, and runs the epilogue.
+// Every sum is taken in a fixed order (within a quad, the scan's fixed tree,
+// then chunk order), so results are reproducible run to run; the order
+// differs from spmv_run's, so the bits do too.
+constexpr int kWinQuads = kBlockNnz / 4 + 1;          // quads of a STREAM block's 4-aligned window
+constexpr int kSegPos = 4 * kWinQuads;                // window positions
+// Dynamic shared memory of the iteration kernels with segmented STREAM blocks
+// (the row parts at their window positions; LONG / CHUNK blocks keep
+// spmv_run's layout, which is larger).
+template <class V>
+constexpr size_t spmv_seg_smem_bytes() {
+    return sizeof(V) * kSegPos > spmv_smem_bytes<1, V>() ? sizeof(V) * kSegPos : spmv_smem_bytes<1, V>();
+}
+
+template <class M, class V, bool NC, class Gather, class Epi>
+__device__ __forceinline__ void spmv_run_seg(const CsrView<M>& A, int cta, const Gather& g, Epi& epi,
+                                             unsigned char* smem) {
+    const RowBlock b = A.blocks[cta];
+    if (!epi.begin(b.inst)) return;  // instance not iterating (uniform over the CTA)
+    if (b.kind != kStream) {
+        long_block<1, M, V>(A, b, g, epi, reinterpret_cast<V*>(smem + sizeof(V) * kProdStride));
+        return;
+    }
+    const unsigned* __restrict__ bits = A.bits + b.slot_base;  // this block's row-start bitmap
+    V* part = reinterpret_cast<V*>(smem);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nrows = b.r1 - b.r0;                                   // <= kThreads
+    const int a = b.p0 & 3, q0 = b.p0 >> 2, nq = ((b.p1 + 3) >> 2) - q0, cnt = b.p1 - b.p0;  // nq <= kWinQuads
+    const bool act = tid < nrows;
+    const int nchunks = (nq + 31) >> 5;
+#pragma unroll 1
+    for (int c = warp; c < nchunks; c += kWarps) {  // warp-uniform
+        const int q = 32 * c + lane;                 // this lane's window quad
+        V p[4] = {V(0), V(0), V(0), V(0)};
+        unsigned f = 0u;                             // row starts among the quad's 4 positions
+        if (q < nq) {
+            f = (__ldg(bits + (q >> 3)) >> ((4 * q) & 31)) & 0xFu;
+            int js[4];
+            M a4[4];
+            if (A.vec) {
+                int4 j4;
+                if constexpr (NC) {
+                    j4 = ld_stream(reinterpret_cast<const int4*>(A.idx) + q0 + q);
+                    load4_stream(A.val + 4 * (q0 + q), a4);
+                } else {
+                    j4 = __ldg(reinterpret_cast<const int4*>(A.idx) + q0 + q);
+                    load4(A.val + 4 * (q0 + q), a4);
+                }
+                js[0] = j4.x; js[1] = j4.y; js[2] = j4.z; js[3] = j4.w;
+            } else {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int k = 4 * q + u - a;
+                    js[u] = (k >= 0 && k < cnt) ? __ldg(A.idx + b.p0 + k) : 0;
+                    a4[u] = (k >= 0 && k < cnt) ? __ldg(A.val + b.p0 + k) : M(0);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = 4 * q + u - a;
+                if (k >= 0 && k < cnt) {
+                    V xv[1];
+                    g(js[u], xv);
+                    p[u] = static_cast<V>(a4[u]) * xv[0];
+                }
+            }
+        }
+        // segmented prefix inside the quad; `v` = the lane's open part at its end
+        V v = V(0);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if ((f >> u) & 1u) v = V(0);
+            v += p[u];
+            p[u] = v;
+        }
+        // segmented inclusive scan over the lanes: a lane adds its left
+        // neighbour's partial only while no row starts in between
+        const unsigned heads = __ballot_sync(0xffffffffu, f != 0u);
+        const unsigned upto_lane = heads & ((2u << lane) - 1u);   // heads in lanes 0..lane
+        const int hl = upto_lane ? 31 - __clz(upto_lane) : -1;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const V pv = __shfl_up_sync(0xffffffffu, v, d);
+            if (lane - d >= hl && lane >= d) v = pv + v;
+        }
+        V cin = __shfl_up_sync(0xffffffffu, v, 1);
+        if (lane == 0) cin = V(0);
+        const unsigned first = __ballot_sync(0xffffffffu, (f & 1u) != 0u);  // lanes whose quad opens with a start
+        const bool next_starts = lane < 31 && ((first >> (lane + 1)) & 1u) != 0u;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (!(f & ((2u << u) - 1u))) p[u] = cin + p[u];  // no start up to u in this quad
+            const int k = 4 * q + u - a;
+            const bool end = (u < 3 ? ((f >> (u + 1)) & 1u) != 0u : (lane == 31 || next_starts)) || k == cnt - 1;
+            if (end && k >= 0 && k < cnt) part[4 * q + u] = p[u];
+        }
+    }
+    // the rows' bounds and epilogue operands are loaded only now (holding them
+    // through the chunk loop costs the 32-register kernels spills); their
+    // latency overlaps the barrier
+    int s = 0, e = 0;
+    decltype(epi.prefetch(0)) pre{};
+    if (act) {
+        s = __ldg(A.ptr + b.r0 + tid) - b.p0;
+        e = __ldg(A.ptr + b.r0 + tid + 1) - b.p0;
+        pre = epi.prefetch(b.r0 + tid);
+    }
+    __syncthreads();
+    if (act) {
+        V tot[1] = {V(0)};
+        if (e > s) {
+            const int pe = e - 1 + a, cs = (s + a) >> 7, ce = pe >> 7;
+            tot[0] = part[min(pe, 128 * cs + 127)];
+            for (int cc = cs + 1; cc <= ce; ++cc) tot[0] += part[min(pe, 128 * cc + 127)];
+        }
+        epi(b.r0 + tid, tot, pre);
+    }
+}
+
+// STREAM-block reduction of the iteration kernels, by vector type.  Measured
+// on B200 (CUDA graphs of back-to-back launches, 512-LP batch / blending LP):
+// the segmented form is 11% / 3% faster per FP64 iteration (87.0 vs 98.2 µs,
+// 28.2 vs 29.1 µs) and the same / 9% slower per FP32 iteration (53.2 vs
+// 53.6 µs, 17.1 vs 15.7 µs) as staging the products in shared memory.
+template <class M, class V, bool NC, class Gather, class Epi>
+__device__ __forceinline__ void spmv_run_iter(const CsrView<M>& A, int cta, const Gather& g, Epi& epi,
+                                              unsigned char* smem) {
+    if constexpr (sizeof(V) == 8) spmv_run_seg<M, V, NC>(A, cta, g, epi, smem);
+    else spmv_run<1, M, V, NC>(A, cta, g, epi, smem);
+}
+
 // Load mode kLoadPrefetch of the iteration kernels (which must NOT call
 // pdl_enter themselves): the schedule and the matrix are written once at
 // set-up, so before the programmatic-launch wait one thread reads the CTA's
@@ -458,8 +634,8 @@ __device__ __forceinline__ void spmv_run(const CsrView<M>& A, int cta, const Gat
 // prefetching vectors that the previous kernel may still be writing is only
 // a hint, never a stale read.  epi.hint(inst) may read stale per-instance
 // state (it runs before the wait) and must only err towards true.  Results
-// are bit-identical to spmv_run.
-template <int NV, class M, class V, class Gather, class Epi>
+// are bit-identical to spmv_run_seg's.
+template <class M, class V, class Gather, class Epi>
 __device__ __forceinline__ void spmv_run_prefetched(const CsrView<M>& A, int cta, const Gather& g, Epi& epi,
                                                     unsigned char* smem) {
     if (threadIdx.x == 0) {
@@ -472,7 +648,7 @@ __device__ __forceinline__ void spmv_run_prefetched(const CsrView<M>& A, int cta
         }
     }
     pdl_enter();
-    spmv_run<NV, M, V, true>(A, cta, g, epi, smem);
+    spmv_run_iter<M, V, true>(A, cta, g, epi, smem);
 }
 
 }  // namespace gb

@@ -424,7 +424,12 @@ int gb_strong_branch(const gb_lp* lp, const double* x, const double* y, int32_t 
  * (B^T y_D = c_F, B x_F = b_D - A[D,N] x_N, B = A[D,F]), solved per instance by
  * MINRES; the vertex it gives replaces the PDHG point when it certifies
  * better in FP64 (OSQP-style polishing).  A polished start is a fixed point of
- * the PDHG map, so the tail then reproduces it.
+ * the PDHG map, so the tail then reproduces it.  When that reduced system
+ * does not converge and the active set is not square (|D| != |F|, impossible
+ * at a nondegenerate vertex: a dual or a slack within the tolerance of zero
+ * was misread), the excess rows leave D smallest |y| first (equality rows
+ * stay) or the excess free columns go to their nearest finite bound, and the
+ * system is solved again (info.active_set_repaired).
  * Backward: given dL/dx* and dL/dy*, exact reverse mode through the K tail
  * iterations (each R-segment recomputed from its checkpoint; projections,
  * extrapolation and the scaling are differentiated), then -- unless switched
@@ -432,7 +437,9 @@ int gb_strong_branch(const gb_lp* lp, const double* x, const double* y, int32_t 
  * fixed point of the PDHG map: a per-instance MINRES solve on the projection
  * masks of that point (for a nondegenerate vertex this is the basis
  * sensitivity).  Returns dL/dc, dL/dlo, dL/dhi and dL/d(A values) (CSR order
- * of the input A) in original units; scaling factors are held constant. */
+ * of the input A) in original units; scaling factors are held constant.
+ * An instance whose completion did not converge (info.implicit_converged = 0)
+ * gets NaN in all of its gradient entries rather than an unverified value. */
 typedef struct gb_diff gb_diff;
 typedef struct {
     int64_t implicit_max_iters;     /* MINRES steps per instance at most (0: truncated gradient,
@@ -453,6 +460,8 @@ typedef struct {
     int32_t free_cols;              /* columns strictly inside their box at the tail start (-1: unknown) */
     int32_t active_rows;            /* rows whose dual is not projected to 0 there (-1: unknown) */
     int32_t polished;               /* the tail started from the polished vertex */
+    int32_t active_set_repaired;    /* polishing repaired a non-square active set (see gb_diff_forward) */
+    int32_t pad;
     int64_t polish_iterations;      /* MINRES steps of the polishing solve */
     int64_t launches;               /* kernel launches of the last forward / backward call */
 } gb_diff_info;
