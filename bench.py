@@ -479,7 +479,8 @@ def batch_measure(dist, rank: int, world: int, steps: int = 3) -> dict:
             "bf16_trial": {"lps_per_s": len(lps) / t_bf, "certified_1e-4": int(cert_bf),
                            "ms_per_iter_bf16": ktb["ms_primal"] + ktb["ms_dual"],
                            "gbs_bf16": ktb["bytes_per_iter"] / ((ktb["ms_primal"] + ktb["ms_dual"]) / 1e3) / 1e9},
-            "autotune": {"seconds": tune_s, "ms_per_iter_default": tune["ms_per_iter_default"],
+            "autotune": {"seconds": tune_s, "load_modes": tune["load_modes"],
+                         "ms_per_iter_default": tune["ms_per_iter_default"],
                          "ms_per_iter_tuned": tune["ms_per_iter_tuned"],
                          "ms_per_iter_default_f64": tune["ms_per_iter_default_f64"],
                          "ms_per_iter_tuned_f64": tune["ms_per_iter_tuned_f64"],
@@ -495,14 +496,15 @@ def batch_measure(dist, rank: int, world: int, steps: int = 3) -> dict:
             "timing": "host wall clock around gb_batch_solve (synchronous), best of %d, max over ranks" % steps}
 
 
-def diff_measure(dist, rank: int, world: int, count: int = 256, steps: int = 2, check: int = 2) -> dict:
+def diff_measure(dist, rank: int, world: int, count: int = 256, steps: int = 2, check: int = 16) -> dict:
     """Differentiable batched LP layer: `count` nondegenerate LPs of m=500,
     n=1000, 10 nnz/col (the random-LP family with a unique strictly
     complementary optimum; workloads.diff_batch), forward = mixed-precision
     restarted PDHG to 1e-6 + polishing + K=200 tail iterations checkpointed
     every R=20, backward = reverse pass + implicit completion for
-    L = w.x* + v.y*.  Gradients of `check` instances are compared with the
-    exact basis sensitivities of their constructed optimal vertex."""
+    L = w.x* + v.y*.  Gradients of the first `check` instances are compared
+    with the exact basis sensitivities of the reference dual simplex's optimal
+    bases."""
     import torch
 
     import ganit_v2_b200 as gb
@@ -544,15 +546,19 @@ def diff_measure(dist, rank: int, world: int, count: int = 256, steps: int = 2, 
     mr_max = reduce_max(dist, max(i["implicit_iterations"] for i in infos))
     its_max = reduce_max(dist, max(r.iterations for r in res))
     errs = []
-    if rank == 0:
-        # exact sensitivities of the constructed vertex (workloads.nondegenerate_lp
-        # builds each instance around a known nonsingular basis B = A[tight, interior])
+    if rank == 0 and world == 1:
+        # exact basis sensitivities of the reference dual simplex's optimal bases
+        # (tests/golden/diff_bases.npz, make_diff_bases.py) for the first instances
+        ref = np.load(os.path.join(ROOT, "tests", "golden", "diff_bases.npz"))
         n0, m0, z0 = ds.n_off, ds.m_off, ds.nnz_off
-        for i in range(min(check, len(mine))):
+        for i in range(min(check, len(ref["heads"]), len(mine))):
             lp = mine[i]
+            head = ref["heads"][i]
+            basic = np.sort(head[head < lp.n])
+            act = np.ones(lp.m, dtype=bool)
+            act[head[head >= lp.n] - lp.n] = False
+            X, Y = ref["x"][i], ref["y"][i]
             A = lp.A.to_scipy().tocsr()
-            basic, act = np.flatnonzero(lp.meta["interior"]), lp.meta["tight"]
-            X, Y = lp.meta["x0"], lp.meta["y0"]
             B = A[np.flatnonzero(act)][:, basic].toarray()
             wi, vi = w[n0[i]:n0[i + 1]], v[m0[i]:m0[i + 1]]
             p = np.zeros(lp.m)
@@ -574,8 +580,8 @@ def diff_measure(dist, rank: int, world: int, count: int = 256, steps: int = 2, 
                                                    "max_c": max((e[0] for e in errs), default=None),
                                                    "max_b": max((e[1] for e in errs), default=None),
                                                    "max_A": max((e[2] for e in errs), default=None)},
-            "grad_checks": "vs the constructed basis here; vs the reference dual simplex and central differences "
-                           "(h=1e-4) of its exact solution map in tests/test_gpu_diff.py",
+            "grad_checks": "vs the basis sensitivities of the reference dual simplex's optimal bases of the first "
+                           "instances (tests/golden/diff_bases.npz); central differences in tests/test_gpu_diff.py",
             "parallelism": f"instances split over {world} GPUs (nnz-balanced)" if world > 1 else "single GPU",
             "timing": f"host wall clock around gb_diff_forward / gb_diff_backward (synchronous), best of {steps}, "
                       "max over ranks"}
@@ -664,6 +670,10 @@ def main():
             launches += prob.stats()[0]
         return total, res, launches
 
+    prob.solve(mixed, fetch=False)
+    t0 = time.perf_counter()
+    tune = prob.autotune(30)  # row cuts and load variants of the iteration kernels (setup, untimed)
+    tune_s = time.perf_counter() - t0
     for _ in range(args.warmup):
         prob.solve(mixed, fetch=False)
         prob.solve(fp64, fetch=False)
@@ -822,6 +832,10 @@ def main():
                     "status": re2e.status_name, "setup_s_last": re2e.setup_seconds, "solve_s_last": re2e.solve_seconds,
                     "note": "gb_solve: pinned host arrays in, upload + validation + device scaling + solve + "
                             "FP64 certification + download into pinned arrays"},
+            "autotune": {"seconds": tune_s, **tune,
+                         "note": "the resident problem's iteration kernels after gb_problem_autotune (row-block cuts, "
+                                 "load variant per matrix); `value` and the kernel timings use them, the one-shot "
+                                 "`e2e` call does not tune"},
             "gpu_launches": launches,
             "clocks": clk,
             "cpu_baseline": cpu,

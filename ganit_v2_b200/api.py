@@ -163,6 +163,14 @@ class GbKkt(C.Structure):
                 ("rel_gap", C.c_double), ("err", C.c_double)]
 
 
+LOAD_MODES = {0: "plain", 1: "stream", 2: "prefetch"}  # GB_LOAD_*
+
+
+def _load_mode_names(m) -> dict:
+    return {"A_f32": LOAD_MODES[int(m[0])], "AT_f32": LOAD_MODES[int(m[1])], "A_f64": LOAD_MODES[int(m[2])],
+            "AT_f64": LOAD_MODES[int(m[3])]}
+
+
 # Every symbol of include/ganit_b200.h (checked by the tests).
 EXPORTS = [
     "gb_last_error", "gb_release_cached_memory", "gb_cached_memory_bytes", "gb_version", "gb_default_options", "gb_set_device", "gb_solve", "gb_problem_create",
@@ -177,7 +185,8 @@ EXPORTS = [
     "gb_diff_default_options", "gb_diff_set_options", "gb_diff_backward", "gb_diff_get_info", "gb_diff_tail_start", "gb_diff_destroy",
     "gb_eval_kkt_noalloc", "gb_read_mps", "gb_model_lp", "gb_model_name", "gb_model_free", "gb_factor_detect",
     "gb_factor_lp", "gb_factor_expand", "gb_factor_free", "gb_model_is_int", "gb_strong_branch",
-    "gb_problem_set_start", "gb_batch_set_start", "gb_batch_clear_start",
+    "gb_problem_set_start", "gb_batch_set_start", "gb_batch_clear_start", "gb_batch_load_modes",
+    "gb_problem_load_modes",
 ]
 
 _lib = None
@@ -214,6 +223,7 @@ def load_library(path: str = LIB_PATH):
         "gb_batch_create": (i32, [i32, vp, vp, vp]), "gb_batch_solve": (i32, [vp, vp, vp]),
         "gb_batch_get_solution": (i32, [vp, i32, vp, vp]), "gb_batch_schedule": (i32, [vp, vp, vp, vp]),
         "gb_batch_autotune": (i32, [vp, i32, vp, vp, vp, vp]),
+        "gb_batch_load_modes": (i32, [vp, vp]), "gb_problem_load_modes": (i32, [vp, vp]),
         "gb_batch_time_kernels": (i32, [vp, i32, i32, vp, vp, vp, vp]),
         "gb_batch_destroy": (None, [vp]), "gb_diff_create": (i32, [i32, vp, vp, i32, i32, vp]),
         "gb_diff_forward": (i32, [vp, vp, vp, vp, vp]), "gb_diff_default_options": (None, [vp]),
@@ -535,7 +545,14 @@ class Problem:
         _check(self._lib.gb_problem_autotune(self._h, int(iters), _p(bn), _p(mr), _p(t0), _p(t1)))
         return {"block_nnz": int(bn[0]), "max_rows": int(mr[0]), "ms_per_iter_default": float(t0[0]),
                 "ms_per_iter_tuned": float(t1[0]), "block_nnz_f64": int(bn[1]), "max_rows_f64": int(mr[1]),
-                "ms_per_iter_default_f64": float(t0[1]), "ms_per_iter_tuned_f64": float(t1[1])}
+                "ms_per_iter_default_f64": float(t0[1]), "ms_per_iter_tuned_f64": float(t1[1]),
+                "load_modes": self.load_modes()}
+
+    def load_modes(self) -> dict:
+        """Load variant per matrix and precision class (gb_problem_load_modes)."""
+        m = np.zeros(4, dtype=np.int32)
+        _check(self._lib.gb_problem_load_modes(self._h, _p(m)))
+        return _load_mode_names(m)
 
     def time_kernels_graph(self, level: int, iters: int = 200) -> dict:
         """Back-to-back launches captured in CUDA graphs (gb_problem_time_kernels_graph)."""
@@ -637,7 +654,14 @@ class BatchSolver:
         _check(self._lib.gb_batch_autotune(self._h, int(iters), _p(bn), _p(mr), _p(t0), _p(t1)))
         return {"block_nnz": bn[:k], "max_rows": mr[:k], "block_nnz_f64": bn[k:], "max_rows_f64": mr[k:],
                 "ms_per_iter_default": float(t0[0]), "ms_per_iter_tuned": float(t1[0]),
-                "ms_per_iter_default_f64": float(t0[1]), "ms_per_iter_tuned_f64": float(t1[1])}
+                "ms_per_iter_default_f64": float(t0[1]), "ms_per_iter_tuned_f64": float(t1[1]),
+                "load_modes": self.load_modes()}
+
+    def load_modes(self) -> dict:
+        """Load variant per matrix and precision class (gb_batch_load_modes)."""
+        m = np.zeros(4, dtype=np.int32)
+        _check(self._lib.gb_batch_load_modes(self._h, _p(m)))
+        return _load_mode_names(m)
 
     def time_kernels(self, level: int = 0, iters: int = 50) -> dict:
         """Device time of the fused iteration kernels with every instance active."""

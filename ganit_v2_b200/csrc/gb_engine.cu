@@ -477,6 +477,7 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
         const int forced = load_mode_override();
         const int nc = forced >= 0 ? forced : (iter > kL2StreamBytes ? kLoadStream : kLoadPlain);
         P->A.stream_nc[w] = P->AT.stream_nc[w] = nc;
+        P->A.default_nc[w] = P->AT.default_nc[w] = nc;
     }
     if (P->has_q && !P->dplr) cvt32(P->Q);
     convert_data(*P, P->v32, s);
@@ -1023,6 +1024,7 @@ void time_level(Problem& P, int iters, double* msp, double* msd, int64_t* launch
 // launch, as the solve loop issues them, and the graph timed with two CUDA
 // events), and of one full iteration (the pair, alternating buffers).  Every
 // instance is active.  Warm L2: the same matrix and vectors every launch.
+// msp / msd may be NULL (only the iteration is timed then).
 template <class M, class V>
 void time_level_graph(Problem& P, int iters, double* msp, double* msd, double* msi) {
     cudaStream_t s = P.stream;
@@ -1067,12 +1069,14 @@ void time_level_graph(Problem& P, int iters, double* msp, double* msd, double* m
         cudaGraphDestroy(g);
         return static_cast<double>(ms) / iters;
     };
-    *msp = timed_graph([&](cudaStream_t cs) {
-        for (int k = 0; k < iters; ++k) launch_primal<M, V>(pa, cs);
-    });
-    *msd = timed_graph([&](cudaStream_t cs) {
-        for (int k = 0; k < iters; ++k) launch_dual<M, V>(da, cs);
-    });
+    if (msp)
+        *msp = timed_graph([&](cudaStream_t cs) {
+            for (int k = 0; k < iters; ++k) launch_primal<M, V>(pa, cs);
+        });
+    if (msd)
+        *msd = timed_graph([&](cudaStream_t cs) {
+            for (int k = 0; k < iters; ++k) launch_dual<M, V>(da, cs);
+        });
     *msi = timed_graph([&](cudaStream_t cs) {
         long long nl = 0;
         for (int k = 0; k < iters; ++k) launch_iteration<M, V>(P, vs, k, cs, nl);
@@ -1142,14 +1146,13 @@ void autotune_class(Problem& P, int w, int iters, double* ms_default, double* ms
         b = (b + 31) / 32 * 32;
         if (b >= 256 && b <= kBlockNnz) cand.push_back({static_cast<int>(b), kThreads});
     }
-    auto measure = [&]() {
+    auto measure = [&]() {  // ms per iteration, back to back in a CUDA graph as the solve loop issues them
         double best = INFINITY;
         for (int rep = 0; rep < 2; ++rep) {
-            double mp = 0, md = 0;
-            int64_t nl = 0;
-            if (w == 0) time_level<float, float>(P, iters, &mp, &md, &nl);
-            else time_level<double, double>(P, iters, &mp, &md, &nl);
-            best = std::min(best, mp + md);
+            double mi = 0;
+            if (w == 0) time_level_graph<float, float>(P, iters, nullptr, nullptr, &mi);
+            else time_level_graph<double, double>(P, iters, nullptr, nullptr, &mi);
+            best = std::min(best, mi);
         }
         return best;
     };
@@ -1157,9 +1160,29 @@ void autotune_class(Problem& P, int w, int iters, double* ms_default, double* ms
     auto& tr = P.tune_max_rows[w];
     tb.assign(P.count, kBlockNnz);
     tr.assign(P.count, kThreads);
+    P.A.stream_nc[w] = P.A.default_nc[w];
+    P.AT.stream_nc[w] = P.AT.default_nc[w];
     rebuild_schedules(P, w);
     double best = measure();
     if (ms_default) *ms_default = best;
+    // load mode of each matrix's kernel (k_dual reads A, k_primal A^T), the
+    // other at its incumbent
+    for (DevMat* mat : {&P.A, &P.AT}) {
+        const int inc = mat->stream_nc[w];
+        int win = inc;
+        for (int mode : {kLoadPlain, kLoadStream, kLoadPrefetch}) {
+            if (mode == inc) continue;
+            mat->stream_nc[w] = mode;
+            for (auto& g : P.graphs) g.reset();
+            const double t = measure();
+            if (t < 0.99 * best) {
+                best = t;
+                win = mode;
+            }
+        }
+        mat->stream_nc[w] = win;
+        for (auto& g : P.graphs) g.reset();
+    }
     std::vector<int> order(P.count);
     std::iota(order.begin(), order.end(), 0);
     auto nnz_of = [&](int k) { return static_cast<long long>(P.nnz_off[k + 1]) - P.nnz_off[k]; };
@@ -1457,6 +1480,27 @@ int gb_batch_schedule(gb_batch* b, int* threads, int* blocks_per_sm, int* groups
                 groups[2 * k + 1] = mode_g(bt, sb.host_seg_block[k], sb.host_seg_block[k + 1]);
             }
         }
+    });
+}
+
+static void load_modes_of(const Problem& P, int* modes) {
+    modes[0] = P.A.stream_nc[0];
+    modes[1] = P.AT.stream_nc[0];
+    modes[2] = P.A.stream_nc[1];
+    modes[3] = P.AT.stream_nc[1];
+}
+
+int gb_batch_load_modes(gb_batch* b, int* modes) {
+    return guarded([&] {
+        GB_REQUIRE(b != nullptr && modes != nullptr, "null argument");
+        load_modes_of(*b->p, modes);
+    });
+}
+
+int gb_problem_load_modes(gb_problem* p, int* modes) {
+    return guarded([&] {
+        GB_REQUIRE(p != nullptr && modes != nullptr, "null argument");
+        load_modes_of(*p->p, modes);
     });
 }
 

@@ -23,6 +23,7 @@ struct DevMat {
     DevSchedule sched;    // row blocks of the FP64-matrix kernels (and of all kernels until tuned)
     DevSchedule sched32;  // row blocks tuned for the FP32 / BF16-matrix kernels (empty: use sched)
     int stream_nc[2] = {0, 0};  // CsrView::nc (LoadMode) for the FP32 / BF16 views and for the FP64 view
+    int default_nc[2] = {0, 0}; // the untuned choice (from the iteration's bytes against the L2)
     std::vector<int> host_ptr;
     // The schedule the kernels of matrix type M run on: FP32 and BF16 kernels
     // keep more CTAs resident per SM than FP64 ones, so the best cut differs.

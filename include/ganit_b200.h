@@ -308,6 +308,18 @@ int gb_batch_schedule(gb_batch* b, int* threads, int* blocks_per_sm, int* groups
  * (arrays of 2 * count: FP32 schedule then FP64; may be NULL) and the
  * per-iteration kernel time of the default and tuned schedules (ms, [2]). */
 int gb_batch_autotune(gb_batch* b, int iters, int* block_nnz, int* max_rows, double* ms_default, double* ms_tuned);
+/* Load variant of the fused iteration kernels, per matrix and precision
+ * class: modes[0..3] = A (FP32/BF16 kernels), A^T (FP32/BF16), A (FP64),
+ * A^T (FP64); GB_LOAD_PLAIN: 16-byte idx / value loads through L1;
+ * GB_LOAD_STREAM: the same loads without L1 allocation; GB_LOAD_PREFETCH:
+ * the streaming loads after a bulk L2 prefetch of each row block's window,
+ * issued before the kernel waits for its predecessor.  Untuned, a matrix
+ * streams when an iteration's data exceeds the L2 (126 MB) and loads plainly
+ * otherwise (GANIT_B200_LOADS=plain|stream|prefetch forces one); the
+ * autotuners time all three per matrix and keep the fastest. */
+enum { GB_LOAD_PLAIN = 0, GB_LOAD_STREAM = 1, GB_LOAD_PREFETCH = 2 };
+int gb_batch_load_modes(gb_batch* b, int* modes);
+int gb_problem_load_modes(gb_problem* p, int* modes);
 /* Average device time of the two fused iteration kernels over `iters`
  * iterations at a precision level (0 = FP32, 1 = FP32 matrix / FP64 vectors,
  * 3 = BF16 matrix / FP32 vectors,
