@@ -281,9 +281,10 @@ def run_profile_qp():
 
 def run_profile_diff():
     """The differentiable layer for ncu: 256 LPs (workloads.diff_batch), one
-    forward (launch it with GANIT_B200_LAUNCH=stream) and one backward.  The
-    forward alone issues ~190,000 launches (PDHG to 1e-6, polishing, the
-    checkpointed tail), so bound any ncu launch list with -s / -c."""
+    forward and one backward.  The PDHG rounds of the forward run as CUDA
+    graphs (ncu sees their kernels only with GANIT_B200_LAUNCH=stream, which
+    turns them into ~50,000 separate launches); the polishing, the tail and
+    the backward are plain launches either way."""
     import numpy as np
 
     import ganit_v2_b200 as gb

@@ -1175,7 +1175,7 @@ void autotune_class(Problem& P, int w, int iters, double* ms_default, double* ms
             mat->stream_nc[w] = mode;
             for (auto& g : P.graphs) g.reset();
             const double t = measure();
-            if (t < 0.99 * best) {
+            if (t < 0.97 * best) {  // 3%: run-to-run noise of one measurement is ~1%
                 best = t;
                 win = mode;
             }
