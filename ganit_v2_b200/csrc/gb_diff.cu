@@ -383,6 +383,15 @@ __global__ void __launch_bounds__(kThreads) k_mr_update(const __grid_constant__ 
     }
 }
 
+// Condition of the MINRES loop graph: repeat while some instance has not finished.
+__global__ void __launch_bounds__(kThreads) k_mr_cond(const MrState* __restrict__ st, int count,
+                                                      unsigned long long cond) {
+    int any = 0;
+    for (int k = threadIdx.x; k < count; k += kThreads) any |= st[k].done == 0;
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) cudaGraphSetConditional(static_cast<cudaGraphConditionalHandle>(cond), any ? 1u : 0u);
+}
+
 // Parameter gradient of T at z_0 against nu: dc' += q, d(lo|hi)' += p, dA' -= p xbar0^T + y0 q^T.
 __global__ void k_implicit_grads(int n, int m, int nnz, const int* __restrict__ row_of, const int* __restrict__ idx,
                                  const i8* __restrict__ cy, const double* __restrict__ q, const double* __restrict__ p,
@@ -498,7 +507,7 @@ __global__ void k_grads_out(int n, int m, int nnz, const int* inst_col, const in
 }
 
 
-constexpr int kMrChunk = 64;  // MINRES steps between host looks at the per-instance flags
+constexpr int kMrChunk = 64;  // MINRES steps between tests of the per-instance flags
 
 }  // namespace
 
@@ -523,6 +532,7 @@ struct Diff {
     int* flags_host = nullptr;
     DevBuf<double> io_n, io_m, io_m2, io_z;
     DevBuf<double> kx, ky;          // vertices certified in an early polishing round (scaled)
+    std::unique_ptr<LevelGraph> mr_graph;  // the MINRES loop (built on first use; fixed buffers)
     std::vector<gb_diff_info> info;
     bool forward_done = false;
     bool backward_done = false;
@@ -595,22 +605,48 @@ struct Diff {
         launches += 1;
         MrOpArgs oa{p.A.view<double>(), p.AT.view<double>(), v};
         const int nb = oa.A.nb + oa.AT.nb;
-        long long steps = 0;
-        while (steps < mr_max) {
+        // The steps run as one CUDA graph: a conditional while node whose body is
+        // kMrChunk steps and a test of the per-instance "done" flags, so the
+        // loop needs no host round trip.  Every instance stops at its own step
+        // bound (MrState::max_it), so the loop ends.
+        if (!mr_graph) {
+            auto g = std::make_unique<LevelGraph>();
+            GB_CUDA(cudaGraphCreate(&g->graph, 0));
+            cudaGraphConditionalHandle h;
+            GB_CUDA(cudaGraphConditionalHandleCreate(&h, g->graph, 1, cudaGraphCondAssignDefault));
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            GB_CUDA(cudaGraphAddNode(&node, g->graph, nullptr, 0, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            cudaStream_t cs;
+            GB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+            GB_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
             for (int c = 0; c < kMrChunk; ++c) {
-                if (nb) k_mr_op<<<nb, kThreads, smem, s>>>(oa);
-                k_mr_update<<<p.count, kThreads, 0, s>>>(v);
+                if (nb) k_mr_op<<<nb, kThreads, smem, cs>>>(oa);
+                k_mr_update<<<p.count, kThreads, 0, cs>>>(v);
             }
-            launches += 2 * kMrChunk;
-            steps += kMrChunk;
-            GB_CUDA(cudaMemcpyAsync(mst_host, mst.get(), sizeof(MrState) * p.count, cudaMemcpyDeviceToHost, s));
-            GB_CUDA(cudaStreamSynchronize(s));
-            bool any = false;
-            for (int k = 0; k < p.count; ++k) any |= mst_host[k].done == 0;
-            if (!any) break;
+            k_mr_cond<<<1, kThreads, 0, cs>>>(mst.get(), p.count, static_cast<unsigned long long>(h));
+            const cudaError_t e = cudaGetLastError();
+            cudaGraph_t done_body = nullptr;
+            const cudaError_t e2 = cudaStreamEndCapture(cs, &done_body);
+            cudaStreamDestroy(cs);
+            if (e != cudaSuccess || e2 != cudaSuccess) {
+                g->graph = nullptr;  // a failed capture: leak the half-built graph rather than destroy it
+                GB_CUDA(e != cudaSuccess ? e : e2);
+            }
+            GB_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
+            mr_graph = std::move(g);
         }
+        GB_CUDA(cudaGraphLaunch(mr_graph->exec, s));
         GB_CUDA(cudaMemcpyAsync(mst_host, mst.get(), sizeof(MrState) * p.count, cudaMemcpyDeviceToHost, s));
         GB_CUDA(cudaStreamSynchronize(s));
+        long long steps = 0;
+        for (int k = 0; k < p.count; ++k) steps = std::max<long long>(steps, mst_host[k].it);
+        launches += ((steps + kMrChunk - 1) / kMrChunk) * (2 * kMrChunk + 1);
     }
 };
 
