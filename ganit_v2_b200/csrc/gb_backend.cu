@@ -173,6 +173,7 @@ struct Vec {
 };
 
 struct Backend {
+    FreeBatchEnd free_batch;  // first member, destroyed last: closes the teardown's free batch
     int device = 0, sms = 148;
     cudaStream_t stream = nullptr;
     int mat_type = GB_F64, vec_type = GB_F64;
@@ -187,7 +188,10 @@ struct Backend {
     DevBuf<double> part, out;
     double* out_host = nullptr;
     ~Backend() {
-        if (out_host) cudaFreeHost(out_host);
+        cudaSetDevice(device);
+        begin_free_batch();
+        free_batch.open = true;
+        host_free(out_host);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -339,7 +343,7 @@ int gb_backend_create(const gb_scaled_lp* s, int mat_type, int vec_type, gb_back
         vec_from_host(B, B.rres, s->rres, s->m);
         B.part.reset(2 * kRedGrid);
         B.out.reset(2);
-        GB_CUDA(cudaMallocHost(&B.out_host, 2 * sizeof(double)));
+        B.out_host = static_cast<double*>(host_alloc(2 * sizeof(double)));
         GB_CUDA(cudaStreamSynchronize(B.stream));
         *out = h.release();
     });

@@ -35,12 +35,49 @@ struct Error : std::runtime_error {
         if (!(cond)) throw ::gb::Error(-1, std::string(msg));        \
     } while (0)
 
+// Stage timer of the set-up and solve paths, on when GANIT_B200_TRACE=1:
+// mark() waits for the stream and prints the host time since the previous
+// mark to stderr (so a stage's time includes its device work).  Off, it does
+// nothing, and no synchronisation is added.
+bool trace_enabled();
+struct StageTrace {
+    cudaStream_t s;
+    const char* what;
+    bool on = trace_enabled();
+    double t = now_ms();
+    static double now_ms();
+    void mark(const char* stage) {
+        if (!on) return;
+        if (s) cudaStreamSynchronize(s);
+        const double u = now_ms();
+        std::fprintf(stderr, "[gb trace] %s %-22s %8.3f ms\n", what, stage, u - t);
+        t = u;
+    }
+};
+
 // Device memory of the library (gb_pool.cu): cudaMalloc / cudaFree behind a
 // per-process cache of freed blocks (same device, same rounded size), so
 // that creating and destroying problems of the same shape -- the one-shot
 // gb_solve path -- does not pay the driver's allocation cost each time.
 void* dev_alloc(size_t bytes);
 void dev_free(void* p);
+// Pinned host memory behind the same kind of cache (a cudaMallocHost /
+// cudaFreeHost pair of a problem's small state arrays measured 1.5-4 ms on
+// the B200 host, as long as the set-up kernels).
+void* host_alloc(size_t bytes);
+void host_free(void* p);
+// A freed block is cached only once no kernel or copy can still use it:
+// dev_free / host_free synchronise the device first, unless a free batch is
+// open on this thread -- a teardown that synchronised once and then frees
+// many buffers (FreeBatch, destroyed last).
+void begin_free_batch();
+void end_free_batch();
+struct FreeBatchEnd {
+    bool open = false;
+    ~FreeBatchEnd() {
+        if (open) end_free_batch();
+    }
+};
 
 // Owning device buffer (move-only).
 template <class T>

@@ -513,6 +513,7 @@ constexpr int kMrChunk = 64;  // MINRES steps between tests of the per-instance 
 
 // ---------------------------------------------------------------- host object
 struct Diff {
+    FreeBatchEnd free_batch;        // first member, destroyed last: closes the teardown's free batch
     std::unique_ptr<Problem> P;
     int K = 200, R = 20, nseg = 10;
     long long mr_max = 20000;
@@ -539,8 +540,11 @@ struct Diff {
     long long launches = 0;
 
     ~Diff() {
-        if (mst_host) cudaFreeHost(mst_host);
-        if (flags_host) cudaFreeHost(flags_host);
+        if (P) cudaSetDevice(P->device);
+        begin_free_batch();
+        free_batch.open = true;
+        host_free(mst_host);
+        host_free(flags_host);
     }
 
     size_t n() const { return static_cast<size_t>(P->n); }
@@ -669,8 +673,8 @@ void diff_alloc(Diff& D) {
     for (int k = 0; k < 12; ++k) D.mr[k].reset(k % 2 == 0 ? n : m);
     D.mst.reset(P.count);
     D.flags.reset(P.count);
-    GB_CUDA(cudaMallocHost(&D.mst_host, sizeof(MrState) * P.count));
-    GB_CUDA(cudaMallocHost(&D.flags_host, sizeof(int) * P.count));
+    D.mst_host = static_cast<MrState*>(host_alloc(sizeof(MrState) * P.count));
+    D.flags_host = static_cast<int*>(host_alloc(sizeof(int) * P.count));
     D.info.assign(P.count, gb_diff_info{});
 }
 

@@ -151,7 +151,7 @@ void device_transpose(Problem& P, cudaStream_t s) {
 template <class F, class Post>
 void inst_reduce(Problem& P, bool rows, F f, int slot, Post post, cudaStream_t s) {
     if (P.count == 1) {
-        reduce_to(s, rows ? P.m : P.n, f, P.red_partials.get(), P.scal.get() + slot, post);
+        reduce_to(s, rows ? P.m : P.n, f, P.red_partials.get(), P.red_arrivals.get(), P.scal.get() + slot, post);
     } else {
         launch_pdl(k_seg_red<F, Post>, P.count, kThreads, 0, s,
                    static_cast<const int*>(rows ? P.d_row_off.get() : P.d_col_off.get()), f, P.scal.get() + slot, post);
@@ -172,7 +172,7 @@ void power_iteration(Problem& P, bool q, cudaStream_t s) {
     k_fill<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, 1.0, v);
     inst_reduce(P, false, Sq{v}, S_PW_NORM, PostSqrt{}, s);
     k_power_reset<<<gi, kThreads, 0, s>>>(P.count, sc);
-    k_power_vec<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, P.icol(), sc, v, v);  // v /= ||v||
+    k_power_vec<<<elem_grid(n, P.sms), kThreads, 0, s>>>(n, P.icol(), sc, v, v, 0);  // v /= ||v||
     const size_t sm1 = spmv_smem_bytes<1, double>();
     const int iters = q ? 60 : 50;
     for (int it = 0; it < iters; ++it) {
@@ -186,9 +186,8 @@ void power_iteration(Problem& P, bool q, cudaStream_t s) {
                        static_cast<const double*>(w), z);
         }
         inst_reduce(P, false, Sq{z}, S_PW_NORM, PostSqrt{}, s);
-        launch_pdl(k_power_vec, elem_grid(n, P.sms), kThreads, 0, s, n, P.icol(), static_cast<const double*>(sc),
-                   static_cast<const double*>(z), v);
-        launch_pdl(k_power_flags, gi, kThreads, 0, s, static_cast<int>(P.count), sc);
+        launch_pdl(k_power_vec, elem_grid(n, P.sms), kThreads, 0, s, n, P.icol(), sc, static_cast<const double*>(z), v,
+                   static_cast<int>(P.count));
     }
     k_finish_norms<<<gi, kThreads, 0, s>>>(P.count, P.d_nnz_off.get(), sc, q ? 1 : 0);
 }
@@ -267,6 +266,8 @@ int load_mode_override() {
     return mode;
 }
 
+void prebuild_graphs(Problem& P, const gb_options* opt);
+
 // Upload + device setup (scale_lp + estimate_norm + run_pdhg's start point)
 // of `count` instances.
 Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
@@ -283,6 +284,8 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     init_kernel_attrs();
     GB_CUDA(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
     cudaStream_t s = P->stream;
+    StageTrace tr{s, "setup"};
+    tr.mark("stream");
     P->count = count;
     P->row_off.assign(count + 1, 0);
     P->col_off.assign(count + 1, 0);
@@ -358,6 +361,7 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     up(lo0, vlo, m);
     up(hi0, vhi, m);
     for (int k = 0; k < count; ++k) validate_entries(&lps[k]);  // overlaps the uploads from pinned memory
+    tr.mark("upload+entries");
     for (DevBuf<double>* b : {&P->c, &P->l, &P->u, &P->C, &P->Cres, &P->x64, &P->xr64, &P->xo, &P->work1})
         b->reset(n);
     for (DevBuf<double>* b : {&P->lo, &P->hi, &P->R, &P->Rres, &P->y64, &P->yr64, &P->yo, &P->work2}) b->reset(m);
@@ -369,6 +373,8 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     }
     P->scal.upload(P->scal_host.data(), P->scal_host.size(), s);
     P->red_partials.reset(kRedGrid);
+    P->red_arrivals.reset(1);
+    GB_CUDA(cudaMemsetAsync(P->red_arrivals.get(), 0, sizeof(unsigned), s));
     P->st.reset(count);
     GB_CUDA(cudaMemsetAsync(P->st.get(), 0, sizeof(SolveState) * count, s));
 
@@ -378,7 +384,9 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
         P->tune_max_rows[w].assign(count, kThreads);
     }
     P->A.sched.upload(build_schedule(P->A.host_ptr.data(), m, P->row_off.data(), count), 3, s);
+    tr.mark("allocs+A schedule");
     device_transpose(*P, s);
+    tr.mark("transpose");
 
     // Ruiz equilibration + Pock-Chambolle (scaling.cpp:47-72); row and column
     // factors are per row / column, so the block-diagonal matrix scales every
@@ -425,9 +433,11 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     inst_reduce(*P, true, FiniteBoundSq{lo0.get(), hi0.get()}, S_BNORM, PostSqrt{}, s);
     inst_reduce(*P, false, Sq{c0.get()}, S_CNORM, PostSqrt{}, s);
 
+    tr.mark("scaling");
     // A^T's schedule, built on the host while the scaling kernels run (the
     // power iteration is its first user)
     P->AT.sched.upload(build_schedule(P->AT.host_ptr.data(), n, P->col_off.data(), count), 3, s);
+    tr.mark("A^T schedule");
 
     // Hessian (single problem only)
     const gb_lp& L0 = lps[0];
@@ -457,6 +467,7 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     }
     if (P->has_q) power_iteration(*P, true, s);
     power_iteration(*P, false, s);  // ||A'|| (scaling.cpp:131-155)
+    tr.mark("power iteration");
     // w0 from the scaled data (pdhg_impl.hpp:258-261)
     inst_reduce(*P, false, Sq{P->c.get()}, S_CN, PostSqrt{}, s);
     inst_reduce(*P, true, FiniteBoundSq{P->lo.get(), P->hi.get()}, S_BN, PostSqrt{}, s);
@@ -482,8 +493,13 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     if (P->has_q && !P->dplr) cvt32(P->Q);
     convert_data(*P, P->v32, s);
     convert_data(*P, P->v64, s);
-    GB_CUDA(cudaMallocHost(&P->st_host, sizeof(SolveState) * count));
-    GB_CUDA(cudaMallocHost(&P->phase_flags_host, sizeof(int) * count));
+    // The phase graphs these options run, captured and instantiated on the
+    // host while the set-up kernels above execute.
+    prebuild_graphs(*P, opt);
+    tr.mark("fp32 copies+graphs");
+    P->st_host = static_cast<SolveState*>(host_alloc(sizeof(SolveState) * count));
+    P->phase_flags_host = static_cast<int*>(host_alloc(sizeof(int) * count));
+    tr.mark("pinned state");
     P->phase_flags.reset(count);
     GB_CUDA(cudaMemcpyAsync(P->scal_host.data(), sc, sizeof(double) * P->scal_host.size(), cudaMemcpyDeviceToHost, s));
     GB_CUDA(cudaStreamSynchronize(s));
@@ -715,6 +731,7 @@ LevelGraph* level_graph(Problem& P, int ce) {
     GB_CUDA(cudaStreamEndCapture(cs, &body));
     GB_CUDA(cudaStreamDestroy(cs));
     GB_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
+    GB_CUDA(cudaGraphUpload(g->exec, P.stream));
     g->launches_per_body = nl;
     return g;
 }
@@ -728,6 +745,18 @@ bool host_loop_mode() {
         return v != nullptr && std::string(v) == "stream";
     }();
     return host;
+}
+
+// Graphs of the precision levels a solve with `opt` runs (the BF16 trial
+// level is built on its first use, with its matrix copy).
+void prebuild_graphs(Problem& P, const gb_options* opt) {
+    if (host_loop_mode() || opt->check_every <= 0) return;
+    P.detect_unbounded = opt->detect_unbounded != 0;
+    if (opt->precision != GB_PREC_DOUBLE) {
+        level_graph<float, float>(P, opt->check_every);
+        if (opt->precision == GB_PREC_DYNAMIC) level_graph<float, double>(P, opt->check_every);
+    }
+    level_graph<double, double>(P, opt->check_every);
 }
 
 // Phase set-up of every instance: in_phase / active from flags.
@@ -819,9 +848,13 @@ void run_phase(Problem& P, const gb_options* opt, double tol, int stall_exit, in
             if (!any) break;
         }
     } else {
+        StageTrace tr{s, level_index<M, V>() == 2 ? "phase f64" : "phase"};
+        tr.mark("phase entry");
         LevelGraph* g = level_graph<M, V>(P, opt->check_every);
+        tr.mark("graph build");
         GB_CUDA(cudaGraphLaunch(g->exec, s));
         per_body = g->launches_per_body;
+        tr.mark("graph run");
     }
     k_phase_out<V><<<gv, kThreads, 0, s>>>(P.n, P.m, P.icol(), P.irow(), vs.x0.get(), vs.y0.get(), vs.sumx.get(),
                                           vs.sumy.get(), vs.xr.get(), vs.yr.get(), P.st.get(), P.x64.get(),
@@ -941,6 +974,8 @@ void solve_problem(Problem& P, const gb_options* opt, gb_result* res) {
         collect();
     }
     // Final FP64 certification of the returned points.
+    StageTrace tr{s, "solve"};
+    tr.mark("phases");
     certify(P);
     k_unscale<<<elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s>>>(P.n, P.m, P.icol(), P.irow(), P.x64.get(),
                                                                      P.y64.get(), P.C.get(), P.R.get(),
@@ -948,6 +983,7 @@ void solve_problem(Problem& P, const gb_options* opt, gb_result* res) {
     P.launches += 1;
     GB_CUDA(cudaStreamSynchronize(s));
     GB_CUDA(cudaGetLastError());
+    tr.mark("certify+unscale");
     const double solve_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     for (int k = 0; k < K; ++k) {
         const SolveState& st = P.st_host[k];
@@ -1386,9 +1422,14 @@ int gb_solve(const gb_lp* lp, const gb_options* opt, gb_result* res, double* x_o
         const gb_options* o = opt ? opt : &def;
         std::unique_ptr<Problem> P(create_problem(1, lp, o));
         solve_problem(*P, o, res);
+        StageTrace tr{P->stream, "gb_solve"};
         if (x_out) P->xo.download(x_out, P->n, P->stream);
         if (y_out) P->yo.download(y_out, P->m, P->stream);
         GB_CUDA(cudaStreamSynchronize(P->stream));
+        tr.mark("download");
+        tr.s = nullptr;  // the stream goes with the problem
+        P.reset();
+        tr.mark("teardown");
     });
 }
 

@@ -98,6 +98,7 @@ struct InstanceResult {
 };
 
 struct Problem {
+    FreeBatchEnd free_batch;              // first member, destroyed last: closes the teardown's free batch
     int device = 0, sms = 148;
     cudaStream_t stream = nullptr;
     int count = 1;                        // instances
@@ -116,6 +117,7 @@ struct Problem {
     DevBuf<double> scal;                                // count x kScal per-instance scalars
     std::vector<double> scal_host;
     DevBuf<double> red_partials;
+    DevBuf<unsigned> red_arrivals;        // k_red's arrival counter (re-armed by its last CTA)
     DevBuf<double> x64, y64, xr64, yr64, xo, yo;
     DevBuf<double> x_start, y_start;      // warm start in original units (NaN: default start); empty: none
     DevBuf<double> work1, work2;          // n / m FP64 scratch
@@ -142,9 +144,12 @@ struct Problem {
     const int* irow() const { return count > 1 ? inst_row.get() : nullptr; }
 
     ~Problem() {
+        cudaSetDevice(device);
+        begin_free_batch();  // one device synchronisation for all the buffers freed below
+        free_batch.open = true;
         for (auto& g : graphs) g.reset();
-        if (st_host) cudaFreeHost(st_host);
-        if (phase_flags_host) cudaFreeHost(phase_flags_host);
+        host_free(st_host);
+        host_free(phase_flags_host);
         if (stream) cudaStreamDestroy(stream);
     }
 };

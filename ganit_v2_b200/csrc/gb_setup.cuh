@@ -13,28 +13,37 @@ namespace gb {
 // ---------------------------------------------------------------- deterministic reductions
 constexpr int kRedGrid = 592;  // 4 CTAs per SM, fixed so the summation order is fixed
 
-// Pass 1: each CTA folds a grid-stride slice; pass 2 folds the partials.
-template <class F>
-__global__ void __launch_bounds__(kThreads) k_red1(long long n, F f, double* partials) {
+// One launch, two passes: each CTA folds a grid-stride slice into
+// partials[cta]; the last CTA to arrive folds the partials in CTA order and
+// writes out = post(sum), then re-arms the arrival counter.  The summation
+// order is fixed by kRedGrid alone.
+template <class F, class P>
+__global__ void __launch_bounds__(kThreads) k_red(long long n, F f, double* partials, unsigned* arrivals,
+                                                  double* out, P post) {
     __shared__ double sh[kWarps];
+    __shared__ bool last;
     pdl_enter();
     double acc = 0.0;
     for (long long i = blockIdx.x * (long long)kThreads + threadIdx.x; i < n; i += (long long)gridDim.x * kThreads)
         acc += f(i);
     double v[1] = {acc};
     block_sum<1>(v, sh);
-    if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
-}
-// out = post(sum of partials)
-template <class P>
-__global__ void __launch_bounds__(kThreads) k_red2(int np, const double* partials, double* out, P post) {
-    __shared__ double sh[kWarps];
-    pdl_enter();
-    double acc = 0.0;
-    for (int i = threadIdx.x; i < np; i += kThreads) acc += partials[i];
-    double v[1] = {acc};
-    block_sum<1>(v, sh);
-    if (threadIdx.x == 0) post(v[0], out);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = v[0];
+        __threadfence();  // the partial is visible before the arrival is counted
+        last = atomicAdd(arrivals, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double a = 0.0;
+    for (int i = threadIdx.x; i < static_cast<int>(gridDim.x); i += kThreads) a += __ldcg(partials + i);
+    double w[1] = {a};
+    block_sum<1>(w, sh);
+    if (threadIdx.x == 0) {
+        post(w[0], out);
+        *arrivals = 0u;
+    }
 }
 struct PostSqrt {
     __device__ void operator()(double s, double* out) const { *out = sqrt(s); }
@@ -61,11 +70,10 @@ struct FiniteBoundSq {  // scaling.cpp:15-24
     }
 };
 
+// `partials` holds kRedGrid doubles; `arrivals` is zero between launches.
 template <class F, class P>
-inline void reduce_to(cudaStream_t s, long long n, F f, double* partials, double* out, P post) {
-    launch_pdl(k_red1<F>, kRedGrid, kThreads, 0, s, n, f, partials);
-    launch_pdl(k_red2<P>, 1, kThreads, 0, s, static_cast<int>(kRedGrid), static_cast<const double*>(partials), out,
-               post);
+inline void reduce_to(cudaStream_t s, long long n, F f, double* partials, unsigned* arrivals, double* out, P post) {
+    launch_pdl(k_red<F, P>, kRedGrid, kThreads, 0, s, n, f, partials, arrivals, out, post);
 }
 
 // ---------------------------------------------------------------- plain SpMV (y = A x)
@@ -233,24 +241,23 @@ static __global__ void k_scale_dplr(int n, int k, const double* __restrict__ Cs,
 
 // Power iteration, per instance (scaling.cpp:137-152): v = z / ||z|| unless
 // the instance's iteration stopped or ||z|| == 0 ...
-static __global__ void k_power_vec(int n, const int* inst_col, const double* sc, const double* __restrict__ z,
-                                   double* __restrict__ v) {
+// With `count` > 0 the same launch then records, per instance, lambda = ||z||
+// ("if (nz == 0.0) break; lambda = nz").  The two parts touch the scalars
+// independently: the flag part sets S_PW_STOP only for an instance whose norm
+// is 0, whose columns the vector part leaves alone whichever value it reads.
+static __global__ void k_power_vec(int n, const int* inst_col, double* sc, const double* z, double* v, int count) {
     pdl_enter();
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const double* s = sc + static_cast<size_t>(inst_of(inst_col, j)) * kScal;
         const double nz = s[S_PW_NORM];
         if (s[S_PW_STOP] == 0.0 && nz != 0.0) v[j] = z[j] / nz;
     }
-}
-// ... then lambda = ||z|| ("if (nz == 0.0) break; lambda = nz").
-static __global__ void k_power_flags(int count, double* sc) {
-    pdl_enter();
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= count) return;
-    double* s = sc + static_cast<size_t>(k) * kScal;
-    if (s[S_PW_STOP] != 0.0) return;
-    if (s[S_PW_NORM] == 0.0) s[S_PW_STOP] = 1.0;
-    else s[S_PW_LAMBDA] = s[S_PW_NORM];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        double* s = sc + static_cast<size_t>(k) * kScal;
+        if (s[S_PW_STOP] != 0.0) continue;
+        if (s[S_PW_NORM] == 0.0) s[S_PW_STOP] = 1.0;
+        else s[S_PW_LAMBDA] = s[S_PW_NORM];
+    }
 }
 static __global__ void k_power_reset(int count, double* sc) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;

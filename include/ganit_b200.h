@@ -130,9 +130,12 @@ const char* gb_last_error(void);
 /* Device memory: the library keeps the blocks it frees (per device and
  * size, at most GANIT_B200_POOL_BYTES, default 4 GiB) and reuses them for the
  * next problem of the same shape, because cudaMalloc / cudaFree of a
- * problem's buffers can cost more than its solve.  A block is cached only
- * after a device synchronisation, as cudaFree would do.  Release returns
- * every cached block to the driver; the second call reports their size. */
+ * problem's buffers can cost more than its solve.  The small pinned host
+ * arrays of a problem's state are kept the same way (at most 256 MiB).  A
+ * block is cached only after a device synchronisation, as cudaFree would do
+ * (one per destroyed problem).  Release returns every cached block, device
+ * and pinned host, to the driver; the second call reports the device bytes
+ * cached. */
 void gb_release_cached_memory(void);
 int64_t gb_cached_memory_bytes(void);
 int gb_version(void);                       /* 10000*major + 100*minor + patch */
