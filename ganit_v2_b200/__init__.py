@@ -10,10 +10,10 @@ The compute path is libganit_b200.so (sm_100a); there is no CPU fallback.
 """
 from .lp import LP, Csr
 from .api import (Backend, BatchSolver, DiffSolver, FactorForm, GanitError, Options, Precision, Problem, Result, Status, load_library, set_device,
-                  solve_pdhg_b200, solve_pdhg_gpu, read_mps, LIB_PATH, StrongBranch, strong_branch, fractional,
+                  transpose, solve_pdhg_b200, solve_pdhg_gpu, read_mps, LIB_PATH, StrongBranch, strong_branch, fractional,
                   most_fractional, BRANCH_VAR, BRANCH_TIGHTEN, BRANCH_NODE_INFEASIBLE)
 
 __all__ = ["LP", "Csr", "Backend", "BatchSolver", "DiffSolver", "FactorForm", "GanitError", "Options", "Precision", "Problem", "Result", "Status",
-           "load_library", "set_device", "solve_pdhg_b200", "solve_pdhg_gpu", "read_mps", "LIB_PATH",
+           "load_library", "set_device", "transpose", "solve_pdhg_b200", "solve_pdhg_gpu", "read_mps", "LIB_PATH",
            "StrongBranch", "strong_branch", "fractional", "most_fractional", "BRANCH_VAR", "BRANCH_TIGHTEN",
            "BRANCH_NODE_INFEASIBLE"]

@@ -173,7 +173,7 @@ def _load_mode_names(m) -> dict:
 
 # Every symbol of include/ganit_b200.h (checked by the tests).
 EXPORTS = [
-    "gb_last_error", "gb_release_cached_memory", "gb_cached_memory_bytes", "gb_version", "gb_default_options", "gb_set_device", "gb_solve", "gb_problem_create",
+    "gb_last_error", "gb_release_cached_memory", "gb_cached_memory_bytes", "gb_version", "gb_default_options", "gb_set_device", "gb_csr_transpose", "gb_solve", "gb_problem_create",
     "gb_problem_solve", "gb_problem_get_solution", "gb_problem_destroy", "gb_problem_stream",
     "gb_problem_time_kernels", "gb_problem_stats", "gb_problem_autotune", "gb_problem_time_kernels_graph",
     "gb_batch_time_kernels_graph", "gb_backend_create", "gb_backend_destroy", "gb_vec_zeros",
@@ -204,7 +204,8 @@ def load_library(path: str = LIB_PATH):
     sig = {
         "gb_last_error": (C.c_char_p, []), "gb_release_cached_memory": (None, []),
         "gb_cached_memory_bytes": (i64, []), "gb_version": (i32, []), "gb_default_options": (None, [vp]),
-        "gb_set_device": (i32, [i32]), "gb_solve": (i32, [vp, vp, vp, vp, vp]),
+        "gb_set_device": (i32, [i32]), "gb_csr_transpose": (i32, [i32, i32, vp, vp, vp, vp, vp, vp]),
+        "gb_solve": (i32, [vp, vp, vp, vp, vp]),
         "gb_problem_create": (i32, [vp, vp, vp]), "gb_problem_solve": (i32, [vp, vp, vp]),
         "gb_problem_get_solution": (i32, [vp, vp, vp]), "gb_problem_destroy": (None, [vp]),
         "gb_problem_stream": (vp, [vp]), "gb_problem_time_kernels": (i32, [vp, i32, i32, vp, vp, vp]),
@@ -469,6 +470,19 @@ def cached_memory_bytes() -> int:
 def set_device(device: int) -> None:
     lib = load_library()
     _check(lib.gb_set_device(int(device)))
+
+
+def transpose(a: Csr) -> Csr:
+    """ganit::transpose (include/ganit/lp.hpp:32, src/lp.cpp:55-72) on the
+    device, as the solver builds A^T (gb_csr_transpose): each row of the
+    result lists its entries in increasing source row."""
+    lib = load_library()
+    t_ptr = np.empty(a.cols + 1, dtype=np.int32)
+    t_idx = np.empty(a.nnz, dtype=np.int32)
+    t_val = np.empty(a.nnz, dtype=np.float64)
+    _check(lib.gb_csr_transpose(int(a.rows), int(a.cols), _p(a.ptr), _p(a.idx), _p(a.val), _p(t_ptr), _p(t_idx),
+                                _p(t_val)))
+    return Csr(a.cols, a.rows, t_ptr, t_idx, t_val)
 
 
 def solve_pdhg_gpu(lp: LP, opt: Options | None = None, out=None) -> Result:

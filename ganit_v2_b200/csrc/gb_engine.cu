@@ -105,8 +105,35 @@ void upload_mat(DevMat& M, int rows, int cols, const int* ptr, const int* idx, c
     }
 }
 
-// Device transpose (lp.cpp:55-72): stable radix sort of column keys keeps the
-// entries of every output row in increasing source-row order.
+// Transpose of a rows x cols CSR matrix on the device (lp.cpp:55-72): row_of
+// = source row of each nonzero; perm = the stable order of the column keys,
+// so every output row lists its entries in increasing source row; t_ptr =
+// the exclusive scan of the column counts; t_idx (and t_val when val and
+// t_val are given) gathered through perm.  Column indices must lie in
+// [0, cols).  The scratch buffers stay with the caller until it synchronises.
+struct TransposeScratch {
+    DevBuf<int> cnt, tile_sum;
+    SortScratch sort;
+};
+void transpose_csr(int rows, int cols, int nnz, const int* ptr, const int* idx, const double* val, int* row_of,
+                   int* perm, int* t_ptr, int* t_idx, double* t_val, int sms, TransposeScratch& w, cudaStream_t s) {
+    const int g = elem_grid(std::max<long long>(nnz, static_cast<long long>(rows) * 32), sms);
+    if (rows) k_row_of<<<g, kThreads, 0, s>>>(rows, ptr, row_of);
+    w.cnt.reset(cols + 1);
+    w.tile_sum.reset(scan_tiles(cols + 1));
+    GB_CUDA(cudaMemsetAsync(w.cnt.get(), 0, sizeof(int) * (cols + 1), s));
+    if (nnz) {
+        k_count_cols<<<elem_grid(nnz, sms), kThreads, 0, s>>>(nnz, idx, w.cnt.get());
+        int bits = 0;  // column keys lie in [0, 2^bits)
+        while ((1LL << bits) < cols) ++bits;
+        stable_sort_index(idx, nnz, bits, perm, sms, w.sort, s);
+        k_gather_transpose<<<elem_grid(nnz, sms), kThreads, 0, s>>>(nnz, perm, row_of, val, t_idx, t_val);
+    }
+    exclusive_scan(w.cnt.get(), t_ptr, cols + 1, w.tile_sum.get(), s);
+}
+
+// A^T of a problem: its structure now, its values after the scaling
+// (k_gather_transpose through perm again).
 void device_transpose(Problem& P, cudaStream_t s) {
     const int nnz = static_cast<int>(P.A.nnz), n = P.n, m = P.m;
     P.AT.rows = n;
@@ -117,31 +144,9 @@ void device_transpose(Problem& P, cudaStream_t s) {
     P.AT.ptr.reset(n + 1);
     P.AT.idx.reset(padded_nnz(nnz));
     P.AT.val64.reset(padded_nnz(nnz));
-    const int g = elem_grid(std::max(nnz, m * 32), P.sms);
-    k_row_of<<<g, kThreads, 0, s>>>(m, P.A.ptr.get(), P.row_of.get());
-    DevBuf<int> cnt(n + 1), keys_out, iota;
-    DevBuf<unsigned char> tmp;
-    GB_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int) * (n + 1), s));
-    if (nnz) {
-        k_count_cols<<<elem_grid(nnz, P.sms), kThreads, 0, s>>>(nnz, P.A.idx.get(), cnt.get());
-        keys_out.reset(nnz);
-        iota.reset(nnz);
-        k_iota<<<elem_grid(nnz, P.sms), kThreads, 0, s>>>(nnz, iota.get());
-        size_t tmp_bytes = 0;
-        int bits = 1;
-        while ((1LL << bits) < n) ++bits;
-        GB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, P.A.idx.get(), keys_out.get(), iota.get(),
-                                                P.perm.get(), nnz, 0, bits, s));
-        tmp.reset(tmp_bytes ? tmp_bytes : 1);
-        GB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tmp_bytes, P.A.idx.get(), keys_out.get(), iota.get(),
-                                                P.perm.get(), nnz, 0, bits, s));
-        k_gather_transpose<<<elem_grid(nnz, P.sms), kThreads, 0, s>>>(nnz, P.perm.get(), P.row_of.get(), nullptr,
-                                                                     P.AT.idx.get(), nullptr);
-    }
-    size_t scan_bytes = 0;
-    GB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, cnt.get(), P.AT.ptr.get(), n + 1, s));
-    DevBuf<unsigned char> stmp(scan_bytes ? scan_bytes : 1);
-    GB_CUDA(cub::DeviceScan::ExclusiveSum(stmp.get(), scan_bytes, cnt.get(), P.AT.ptr.get(), n + 1, s));
+    TransposeScratch w;  // released after the synchronisation below
+    transpose_csr(m, n, nnz, P.A.ptr.get(), P.A.idx.get(), nullptr, P.row_of.get(), P.perm.get(), P.AT.ptr.get(),
+                  P.AT.idx.get(), nullptr, P.sms, w, s);
     P.AT.host_ptr.resize(n + 1);
     GB_CUDA(cudaMemcpyAsync(P.AT.host_ptr.data(), P.AT.ptr.get(), sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
     GB_CUDA(cudaStreamSynchronize(s));
@@ -1351,6 +1356,50 @@ int gb_set_device(int device) {
         check_device(device, &sms);
         g_device = device;
         GB_CUDA(cudaSetDevice(device));
+    });
+}
+
+int gb_csr_transpose(int rows, int cols, const int* ptr, const int* idx, const double* val, int* t_ptr, int* t_idx,
+                     double* t_val) {
+    return guarded([&] {
+        GB_REQUIRE(rows >= 0 && cols >= 0 && ptr != nullptr && t_ptr != nullptr, "bad arguments");
+        GB_REQUIRE(ptr[0] == 0, "ptr[0] must be 0");
+        for (int i = 0; i < rows; ++i) GB_REQUIRE(ptr[i + 1] >= ptr[i], "ptr must be non-decreasing");
+        const int nnz = ptr[rows];
+        GB_REQUIRE(nnz < (1 << 30), "more than 2^30 nonzeros");
+        GB_REQUIRE(nnz == 0 || (idx != nullptr && t_idx != nullptr), "idx / t_idx missing");
+        GB_REQUIRE((val == nullptr) == (t_val == nullptr), "val and t_val go together");
+        for (int p = 0; p < nnz; ++p) GB_REQUIRE(idx[p] >= 0 && idx[p] < cols, "column index out of range");
+        int sms;
+        check_device(g_device, &sms);
+        GB_CUDA(cudaSetDevice(g_device));
+        cudaStream_t s;
+        GB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        struct StreamGuard {
+            cudaStream_t s;
+            ~StreamGuard() {
+                cudaStreamSynchronize(s);
+                cudaStreamDestroy(s);
+            }
+        } sg{s};
+        const size_t z = nnz ? nnz : 1;
+        DevBuf<int> d_ptr(rows + 1), d_idx(z), row_of(z), perm(z), d_tptr(cols + 1), d_tidx(z);
+        DevBuf<double> d_val, d_tval;
+        d_ptr.upload(ptr, rows + 1, s);
+        d_idx.upload(idx, nnz, s);
+        if (val) {
+            d_val.reset(z);
+            d_tval.reset(z);
+            d_val.upload(val, nnz, s);
+        }
+        TransposeScratch w;
+        transpose_csr(rows, cols, nnz, d_ptr.get(), d_idx.get(), d_val.get(), row_of.get(), perm.get(),
+                      d_tptr.get(), d_tidx.get(), d_tval.get(), sms, w, s);
+        d_tptr.download(t_ptr, cols + 1, s);
+        d_tidx.download(t_idx, nnz, s);
+        if (val) d_tval.download(t_val, nnz, s);
+        GB_CUDA(cudaStreamSynchronize(s));
+        GB_CUDA(cudaGetLastError());
     });
 }
 

@@ -3,9 +3,7 @@
 // Restates src/scaling.cpp:8-155 and src/lp.cpp:55-72 as GPU kernels so that
 // a problem never round-trips through host memory after its upload.
 #pragma once
-#include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_scan.cuh>
-
+#include "gb_sort.cuh"
 #include "gb_spmv.cuh"
 
 namespace gb {
@@ -99,9 +97,6 @@ static __global__ void k_row_of(int rows, const int* __restrict__ ptr, int* __re
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int r = warp; r < rows; r += nw)
         for (int p = ptr[r] + lane; p < ptr[r + 1]; p += 32) row_of[p] = r;
-}
-static __global__ void k_iota(int n, int* v) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
 }
 static __global__ void k_count_cols(int nnz, const int* __restrict__ idx, int* __restrict__ cnt) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += gridDim.x * blockDim.x)

@@ -142,6 +142,16 @@ int gb_version(void);                       /* 10000*major + 100*minor + patch *
 void gb_default_options(gb_options* opt);
 /* Selects the CUDA device used by handles created afterwards on this thread. */
 int gb_set_device(int device);
+/* Transpose of a rows x cols CSR matrix (replaces ganit::transpose,
+ * include/ganit/lp.hpp:32, src/lp.cpp:55-72), computed on the device the way
+ * the solver builds A^T: every output row lists its entries in increasing
+ * source row, so the result equals the reference's counting transpose.
+ * ptr: rows + 1 non-decreasing offsets from 0; idx: ptr[rows] column indices
+ * in [0, cols) (checked on the host before upload); val / t_val: optional
+ * (both or neither).  Outputs: t_ptr (cols + 1), t_idx and t_val (ptr[rows]).
+ * Synchronous. */
+int gb_csr_transpose(int rows, int cols, const int* ptr, const int* idx, const double* val, int* t_ptr, int* t_idx,
+                     double* t_val);
 
 /* ---------------------------------------------------------------- 1. fused solver */
 /* One-shot solve of a host problem: upload, scale (on the device), restarted

@@ -206,6 +206,24 @@ def eval_kkt(A, AT, c, l, u, lo, hi, rres, cres, x, y, obj_scale, obj_const, bno
     return dict(zip(("pobj", "dobj", "rel_p", "rel_d", "rel_gap", "err"), (float(v) for v in out)))
 
 
+def transpose(a):
+    """lp.cpp:55-72 (ora_transpose): the counting-sort transpose of a Csr."""
+    from ganit_v2_b200.lp import Csr
+    lib = _load(ORACLE_SO)
+    f = lib.ora_transpose
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 6
+    ptr = np.ascontiguousarray(a.ptr, dtype=np.int32)
+    idx = np.ascontiguousarray(a.idx, dtype=np.int32)
+    val = np.ascontiguousarray(a.val, dtype=np.float64)
+    t_ptr = np.empty(a.cols + 1, dtype=np.int32)
+    t_idx = np.empty(max(a.nnz, 1), dtype=np.int32)
+    t_val = np.empty(max(a.nnz, 1), dtype=np.float64)
+    if f(a.rows, a.cols, _p(ptr), _p(idx), _p(val), _p(t_ptr), _p(t_idx), _p(t_val)) != 0:
+        raise MemoryError("ora_transpose")
+    return Csr(a.cols, a.rows, t_ptr, t_idx[:a.nnz], t_val[:a.nnz])
+
+
 # ---------------------------------------------------------------- reference build
 def ref_solve(lp, threads: int | None = None, **opts) -> OracleResult:
     """Run the UNMODIFIED reference ganit::solve_pdhg_cpu (OpenMP; ``threads``

@@ -534,3 +534,19 @@ int ora_eval_kkt(int m, int n, const int* a_ptr, const int* a_idx, const double*
     out[5] = sqrt(rel_p * rel_p + rel_d * rel_d + rel_gap * rel_gap);
     return 0;
 }
+
+/* lp.cpp:55-72 on caller buffers: t_ptr[cols+1], t_idx / t_val[ptr[rows]]. */
+int ora_transpose(int rows, int cols, const int* ptr, const int* idx, const double* val, int* t_ptr, int* t_idx,
+                  double* t_val) {
+    csr_t a, t;
+    if (csr_copy(&a, rows, cols, ptr, idx, val)) { csr_free(&a); return -1; }
+    if (csr_transpose(&a, &t)) { csr_free(&a); csr_free(&t); return -1; }
+    memcpy(t_ptr, t.ptr, sizeof(int) * (size_t)(cols + 1));
+    if (t.nnz) {
+        memcpy(t_idx, t.idx, sizeof(int) * (size_t)t.nnz);
+        memcpy(t_val, t.val, sizeof(double) * (size_t)t.nnz);
+    }
+    csr_free(&a);
+    csr_free(&t);
+    return 0;
+}

@@ -98,6 +98,11 @@ int ora_eval_kkt(int m, int n, const int* a_ptr, const int* a_idx, const double*
                  const double* lo, const double* hi, const double* rres, const double* cres, const double* x,
                  const double* y, const double* sc, double* out);
 
+/* Counting-sort transpose (lp.cpp:55-72) into caller buffers: t_ptr[cols+1],
+ * t_idx / t_val[ptr[rows]].  Checks the device transpose. */
+int ora_transpose(int rows, int cols, const int* ptr, const int* idx, const double* val, int* t_ptr, int* t_idx,
+                  double* t_val);
+
 #ifdef __cplusplus
 }
 #endif
