@@ -383,6 +383,34 @@ __global__ void __launch_bounds__(kThreads) k_mr_update(const __grid_constant__ 
     }
 }
 
+// Per instance: (free columns, dual-active rows) of the codes, one CTA each.
+__global__ void __launch_bounds__(kThreads) k_code_counts(const int* __restrict__ col_off,
+                                                          const int* __restrict__ row_off, const i8* __restrict__ cx,
+                                                          const i8* __restrict__ cy, int2* __restrict__ out) {
+    const int k = blockIdx.x;
+    int f = 0, d = 0;
+    for (int j = col_off[k] + threadIdx.x; j < col_off[k + 1]; j += kThreads) f += cx[j] == 1;
+    for (int i = row_off[k] + threadIdx.x; i < row_off[k + 1]; i += kThreads) d += cy[i] != 0;
+    __shared__ int sf[kWarps], sd[kWarps];
+    for (int o = 16; o > 0; o >>= 1) {
+        f += __shfl_down_sync(0xffffffffu, f, o);
+        d += __shfl_down_sync(0xffffffffu, d, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sf[threadIdx.x >> 5] = f;
+        sd[threadIdx.x >> 5] = d;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tf = 0, td = 0;
+        for (int w = 0; w < kWarps; ++w) {
+            tf += sf[w];
+            td += sd[w];
+        }
+        out[k] = make_int2(tf, td);
+    }
+}
+
 // Condition of the MINRES loop graph: repeat while some instance has not finished.
 __global__ void __launch_bounds__(kThreads) k_mr_cond(const MrState* __restrict__ st, int count,
                                                       unsigned long long cond) {
@@ -531,6 +559,8 @@ struct Diff {
     MrState* mst_host = nullptr;
     DevBuf<int> flags;              // per-instance selection (polish use / restore)
     int* flags_host = nullptr;
+    DevBuf<int2> counts;            // per instance: free columns, dual-active rows of the polishing codes
+    int2* counts_host = nullptr;
     DevBuf<double> io_n, io_m, io_m2, io_z;
     DevBuf<double> kx, ky;          // vertices certified in an early polishing round (scaled)
     std::unique_ptr<LevelGraph> mr_graph;  // the MINRES loop (built on first use; fixed buffers)
@@ -545,6 +575,7 @@ struct Diff {
         free_batch.open = true;
         host_free(mst_host);
         host_free(flags_host);
+        host_free(counts_host);
     }
 
     size_t n() const { return static_cast<size_t>(P->n); }
@@ -675,6 +706,8 @@ void diff_alloc(Diff& D) {
     D.flags.reset(P.count);
     D.mst_host = static_cast<MrState*>(host_alloc(sizeof(MrState) * P.count));
     D.flags_host = static_cast<int*>(host_alloc(sizeof(int) * P.count));
+    D.counts.reset(P.count);
+    D.counts_host = static_cast<int2*>(host_alloc(sizeof(int2) * P.count));
     D.info.assign(P.count, gb_diff_info{});
 }
 
@@ -683,24 +716,23 @@ inline double kkt_err(const Kkt& k) {
     return std::isfinite(e) ? e : INFINITY;
 }
 
-// Active-set repair after a first polishing solve.  An instance whose reduced
-// system did not converge and whose active set is not square (|D| dual-active
-// rows != |F| free columns; a nondegenerate vertex has a square, nonsingular
-// basis B = A'[D, F]) was read off a point whose smallest duals or slacks are
-// within the solve tolerance of zero, so one PDHG step classified them
-// wrongly.  Its excess rows (|D| > |F|) leave D smallest |y+| first (equality
+// Active-set repair before the polishing solve.  An instance whose active set
+// is not square (|D| dual-active rows != |F| free columns; a nondegenerate
+// vertex has a square, nonsingular basis B = A'[D, F]) was read off a point
+// whose smallest duals or slacks are within the solve tolerance of zero, so
+// one PDHG step classified them wrongly, and its reduced system is
+// inconsistent (MINRES would run to its step bound).  Its excess rows (|D| > |F|) leave D smallest |y+| first (equality
 // rows never leave); its excess columns (|F| > |D|) go to their nearest finite
 // bound, nearest first.  The codes are changed in place (they define the
 // reduced system and the polished point) and D.flags selects the repaired
 // instances.  Returns whether any instance was repaired.
-bool repair_active_sets(Diff& D, const std::vector<int>& todo) {
+// `cnt` holds (free columns, dual-active rows) per instance (k_code_counts).
+bool repair_active_sets(Diff& D, const std::vector<int>& todo, const int2* cnt) {
     Problem& P = *D.P;
     cudaStream_t s = P.stream;
     std::vector<int> fix;
-    for (int k = 0; k < P.count; ++k) {
-        const MrState& st = D.mst_host[k];
-        if (todo[k] && !st.converged && st.free_cols != st.active_rows) fix.push_back(k);
-    }
+    for (int k = 0; k < P.count; ++k)
+        if (todo[k] && cnt[k].x != cnt[k].y) fix.push_back(k);
     if (fix.empty()) return false;
     const size_t n = D.n(), m = D.m();
     std::vector<i8> cx(n), cy(m);
@@ -719,7 +751,7 @@ bool repair_active_sets(Diff& D, const std::vector<int>& todo) {
     for (int k : fix) {
         const int c0 = P.col_off[k], c1 = P.col_off[k + 1], r0 = P.row_off[k], r1 = P.row_off[k + 1];
         std::vector<std::pair<double, int>> cand;
-        const int excess = D.mst_host[k].active_rows - D.mst_host[k].free_cols;
+        const int excess = cnt[k].y - cnt[k].x;
         if (excess > 0) {
             for (int i = r0; i < r1; ++i)
                 if (cy[i] != 0 && lo[i] < hi[i]) cand.push_back({std::fabs(y1[i]), i});
@@ -782,14 +814,21 @@ void polish(Diff& D, double accept_tol, const std::vector<int>& todo) {
         }
         D.launches += 2;
     };
+    StageTrace tr{s, "polish"};
+    // A nondegenerate vertex has a square basis (|F| = |D|); a non-square
+    // active set makes the reduced system inconsistent, on which MINRES would
+    // only stop at its step bound, so it is repaired before the solve.
+    k_code_counts<<<P.count, kThreads, 0, s>>>(P.d_col_off.get(), P.d_row_off.get(), D.cx_at(0), D.cy_at(0),
+                                               D.counts.get());
+    GB_CUDA(cudaMemcpyAsync(D.counts_host, D.counts.get(), sizeof(int2) * P.count, cudaMemcpyDeviceToHost, s));
+    GB_CUDA(cudaStreamSynchronize(s));
+    repair_active_sets(D, todo, D.counts_host);
     rhs();
     for (int k = 0; k < P.count; ++k) D.flags_host[k] = todo[k];
     D.flags.upload(D.flags_host, P.count, s);
+    tr.mark("step + repair + rhs");
     D.minres(rhs_x, rhs_y, D.flags.get());
-    if (repair_active_sets(D, todo)) {  // second solve on the instances whose active set was repaired
-        rhs();
-        D.minres(rhs_x, rhs_y, D.flags.get());
-    }
+    tr.mark("minres");
     for (int k = 0; k < P.count; ++k) {
         D.flags_host[k] = todo[k] && D.mst_host[k].converged ? 1 : 0;
         if (todo[k]) D.info[k].polish_iterations = D.mst_host[k].it;
@@ -851,9 +890,13 @@ void diff_forward(Diff& D, const gb_options* opt, gb_result* res, double* x_out,
     std::vector<long long> its(K, 0);
     long long launches = 0;
     bool any_kept = false;
+    StageTrace tr{s, "diff forward"};
+    char lab[48];
     for (;;) {
         solve_problem(P, &o, r);
         launches += P.launches;
+        std::snprintf(lab, sizeof lab, "solve to %.0e", o.tol);
+        tr.mark(lab);
         for (int k = 0; k < K; ++k) {
             its[k] += r[k].iterations;
             if (!todo[k]) continue;
@@ -867,6 +910,7 @@ void diff_forward(Diff& D, const gb_options* opt, gb_result* res, double* x_out,
         if (!D.polish) break;
         const bool last = o.tol <= target;
         polish(D, last ? -1.0 : target, todo);
+        tr.mark("polish");
         if (last) break;
         int left = 0;
         for (int k = 0; k < K; ++k) {
@@ -923,6 +967,7 @@ void diff_forward(Diff& D, const gb_options* opt, gb_result* res, double* x_out,
         D.run_segment(D.R);
     }
     D.seg_valid = D.nseg - 1;
+    tr.mark("tail");
     // the layer's output z_K, certified in FP64 and unscaled
     GB_CUDA(cudaMemcpyAsync(P.x64.get(), D.x_at(D.R), nb, cudaMemcpyDeviceToDevice, s));
     GB_CUDA(cudaMemcpyAsync(P.y64.get(), D.y_at(D.R), mb, cudaMemcpyDeviceToDevice, s));

@@ -449,12 +449,12 @@ int gb_strong_branch(const gb_lp* lp, const double* x, const double* y, int32_t 
  * (B^T y_D = c_F, B x_F = b_D - A[D,N] x_N, B = A[D,F]), solved per instance by
  * MINRES; the vertex it gives replaces the PDHG point when it certifies
  * better in FP64 (OSQP-style polishing).  A polished start is a fixed point of
- * the PDHG map, so the tail then reproduces it.  When that reduced system
- * does not converge and the active set is not square (|D| != |F|, impossible
- * at a nondegenerate vertex: a dual or a slack within the tolerance of zero
- * was misread), the excess rows leave D smallest |y| first (equality rows
- * stay) or the excess free columns go to their nearest finite bound, and the
- * system is solved again (info.active_set_repaired).  With polishing on
+ * the PDHG map, so the tail then reproduces it.  When the active set is not
+ * square (|D| != |F|, impossible at a nondegenerate vertex: a dual or a slack
+ * within the tolerance of zero was misread, and the reduced system is
+ * inconsistent), the excess rows leave D smallest |y| first (equality rows
+ * stay) or the excess free columns go to their nearest finite bound before
+ * the solve (info.active_set_repaired).  With polishing on
  * (and implicit_max_iters > 0) and opt->tol below 1e-4, the solve goes in
  * rounds: first to 1e-4; every instance whose polished vertex certifies at
  * opt->tol keeps it; the rest continue, warm-started from their points, at a
