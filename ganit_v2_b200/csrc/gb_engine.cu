@@ -631,6 +631,12 @@ void iteration_args(Problem& P, VecSet<V>& vs, int k, PrimalArgs<M, V>& pa, Dual
                           P.has_q ? vs.qx.get() : nullptr, xout, vs.xbar.get(), vs.sumx.get(), P.st.get()};
     da = DualArgs<M, V>{P.A.view<M>(), vs.xbar.get(), yin, vs.lo.get(), vs.hi.get(), yout, vs.sumy.get(),
                         P.st.get()};
+    if (P.list_level == level_index<M, V>()) {  // a phase of some instances only
+        pa.AT.blocks = P.list_t.get();
+        pa.AT.nb = P.list_nt;
+        da.A.blocks = P.list_a.get();
+        da.A.nb = P.list_na;
+    }
 }
 
 // The fused iteration kernels at their matrix view's load mode (CsrView::nc).
@@ -696,13 +702,23 @@ long long capture_body(Problem& P, int ce, cudaGraphConditionalHandle cond, cuda
 template <class M, class V>
 LevelGraph* level_graph(Problem& P, int ce) {
     constexpr int li = level_index<M, V>();
-    auto& slot = P.graphs[li];
+    const bool lists = P.list_level == li;
+    auto& slot = P.graphs[li + (lists ? 4 : 0)];
     const int ray = P.detect_unbounded && !P.has_q ? 1 : 0;
-    if (slot && slot->check_every == ce && slot->ray == ray) return slot.get();
+    const RowBlock* la = lists ? P.list_a.get() : nullptr;
+    const RowBlock* lt = lists ? P.list_t.get() : nullptr;
+    const int na = lists ? P.list_na : 0, nt = lists ? P.list_nt : 0;
+    if (slot && slot->check_every == ce && slot->ray == ray && slot->list_a == la && slot->list_t == lt &&
+        slot->list_na == na && slot->list_nt == nt)
+        return slot.get();
     slot.reset(new LevelGraph);
     LevelGraph* g = slot.get();
     g->check_every = ce;
     g->ray = ray;
+    g->list_a = la;
+    g->list_t = lt;
+    g->list_na = na;
+    g->list_nt = nt;
     GB_CUDA(cudaGraphCreate(&g->graph, 0));
     cudaGraphConditionalHandle h;
     GB_CUDA(cudaGraphConditionalHandleCreate(&h, g->graph, 1, cudaGraphCondAssignDefault));
@@ -817,6 +833,51 @@ void sync_state(Problem& P) {
     GB_CUDA(cudaStreamSynchronize(P.stream));
 }
 
+// Block lists of a batch phase that only some instances take part in
+// (phase_flags_host): the iteration kernels of level <M,V> then launch the
+// row blocks of those instances alone (copies of their RowBlocks, which carry
+// their own slot and counter indices), instead of every block with the
+// others' CTAs returning at once -- same blocks, same arithmetic, fewer CTAs.
+// Used when the phase's blocks are at most half of all.
+// GANIT_B200_PHASE_LISTS=0 turns it off.
+bool phase_lists_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("GANIT_B200_PHASE_LISTS");
+        return v == nullptr || std::string(v) != "0";
+    }();
+    return on;
+}
+template <class M, class V>
+void set_phase_lists(Problem& P) {
+    P.list_level = -1;
+    if (P.count <= 1 || !phase_lists_enabled()) return;
+    const DevSchedule& sa = P.A.template sched_for<M>();
+    const DevSchedule& st = P.AT.template sched_for<M>();
+    std::vector<RowBlock> la, lt;
+    for (int k = 0; k < P.count; ++k) {
+        if (!P.phase_flags_host[k]) continue;
+        for (int b = sa.host_seg_block[k]; b < sa.host_seg_block[k + 1]; ++b) la.push_back(sa.host_blocks[b]);
+        for (int b = st.host_seg_block[k]; b < st.host_seg_block[k + 1]; ++b) lt.push_back(st.host_blocks[b]);
+    }
+    if (la.empty() || lt.empty() || 2 * (la.size() + lt.size()) > static_cast<size_t>(sa.nb + st.nb)) return;
+    auto put = [&](DevBuf<RowBlock>& d, const std::vector<RowBlock>& h) {
+        if (d.size() < h.size()) d.reset(h.size());  // a buffer only grows: graphs keep their pointer
+        d.upload(h.data(), h.size(), P.stream);
+    };
+    put(P.list_a, la);
+    put(P.list_t, lt);
+    P.list_na = static_cast<int>(la.size());
+    P.list_nt = static_cast<int>(lt.size());
+    P.list_level = level_index<M, V>();
+    if (trace_enabled())
+        std::fprintf(stderr, "[gb trace] phase lists: %d + %d of %d row blocks\n", P.list_na, P.list_nt,
+                     sa.nb + st.nb);
+}
+struct PhaseListsOff {  // the lists end with the phase, also on an error
+    Problem& P;
+    ~PhaseListsOff() { P.list_level = -1; }
+};
+
 template <class M, class V>
 void run_phase(Problem& P, const gb_options* opt, double tol, int stall_exit, int stall_checks, bool first,
                bool has_r) {
@@ -830,6 +891,8 @@ void run_phase(Problem& P, const gb_options* opt, double tol, int stall_exit, in
                             s));
     k_set_phase<<<div_up(P.count, kThreads), kThreads, 0, s>>>(P.count, P.st.get(), P.phase_flags.get(), tol,
                                                                stall_checks, stall_exit, first ? 1 : 0);
+    set_phase_lists<M, V>(P);
+    PhaseListsOff lists_off{P};
     k_phase_in<V><<<gv, kThreads, 0, s>>>(P.n, P.m, P.icol(), P.irow(), P.st.get(), P.x64.get(), P.y64.get(),
                                          P.xr64.get(), P.yr64.get(), has_r ? 1 : 0, vs.x0.get(), vs.y0.get(),
                                          vs.xr.get(), vs.yr.get(), vs.sumx.get(), vs.sumy.get());

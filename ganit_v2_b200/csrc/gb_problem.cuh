@@ -83,6 +83,11 @@ struct LevelGraph {
     cudaGraph_t graph = nullptr;
     int check_every = 0;
     int ray = 0;  // the check also forms A (x - x_r) (unbounded test)
+    // block lists the iteration kernels were captured with (Problem::list_*;
+    // their contents may change between phases, their buffers and lengths not)
+    const RowBlock* list_a = nullptr;
+    const RowBlock* list_t = nullptr;
+    int list_na = 0, list_nt = 0;
     long long launches_per_body = 0;
     ~LevelGraph() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -130,7 +135,15 @@ struct Problem {
     DevBuf<int> phase_flags;              // per-instance flags uploaded for a phase
     int* phase_flags_host = nullptr;      // pinned
     DevBuf<double> partials;
-    std::unique_ptr<LevelGraph> graphs[4];  // levels <f32,f32>, <f32,f64>, <f64,f64>, <bf16,f32>
+    // Phase graphs: levels <f32,f32>, <f32,f64>, <f64,f64>, <bf16,f32>, then the
+    // same four for phases that run on block lists.
+    std::unique_ptr<LevelGraph> graphs[8];
+    // Row blocks of the current phase when only some instances of a batch take
+    // part and their blocks are at most half of all: copies of those
+    // instances' RowBlocks, which the iteration kernels of level list_level
+    // run alone (list_level -1: none).
+    DevBuf<RowBlock> list_a, list_t;
+    int list_na = 0, list_nt = 0, list_level = -1;
     double setup_seconds = 0.0;
     long long launches = 0;               // kernel launches of the last solve
     std::vector<InstanceResult> results;

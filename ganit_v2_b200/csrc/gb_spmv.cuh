@@ -198,8 +198,10 @@ struct DevSchedule {
     int nb = 0;
     int nslots = 0;
     std::vector<int> host_seg_block;
+    std::vector<RowBlock> host_blocks;  // for the block lists of partial phases
     void upload(const Schedule& s, int nv_max, cudaStream_t st) {
         nb = static_cast<int>(s.blocks.size());
+        host_blocks = s.blocks;
         blocks.reset(nb ? nb : 1);
         blocks.upload(s.blocks.data(), nb, st);
         host_seg_block = s.seg_block;
