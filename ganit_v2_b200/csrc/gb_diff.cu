@@ -39,6 +39,7 @@
 #include <memory>
 
 #include "gb_problem.cuh"
+#include "gb_sort.cuh"
 
 namespace gb {
 namespace {
@@ -220,11 +221,15 @@ struct alignas(16) MrState {
     int done, converged, free_cols, active_rows;
 };
 
+// MINRES vectors live in the compact index space of the reduced system:
+// x-part entry c is free column fidx[c], y-part entry r dual-active row
+// didx[r]; instance k owns x-part [col_off[k], col_off[k+1]) and y-part
+// [row_off[k], row_off[k+1]).
 struct MrVecs {
     const int* col_off;
     const int* row_off;
-    const i8* cx;  // column codes of z_0 (1 = free)
-    const i8* cy;  // row codes of z_0 (!= 0 = dual active)
+    const int* fidx;
+    const int* didx;
     double *vx, *vy, *vpx, *vpy, *px, *py, *d1x, *d1y, *d2x, *d2y, *sx, *sy;
     MrState* st;
 };
@@ -239,24 +244,20 @@ __global__ void __launch_bounds__(kThreads) k_mr_init(const __grid_constant__ Mr
     const int k = blockIdx.x;
     if (sel != nullptr && sel[k] == 0) return;
     const int c0 = a.col_off[k], c1 = a.col_off[k + 1], r0 = a.row_off[k], r1 = a.row_off[k + 1];
-    double v[3] = {0.0, 0.0, 0.0};
-    for (int j = c0 + threadIdx.x; j < c1; j += kThreads) {
-        const bool f = a.cx[j] == 1;
-        const double b = f ? mux[j] : 0.0;
-        a.vx[j] = b;
-        a.vpx[j] = a.px[j] = a.d1x[j] = a.d2x[j] = a.sx[j] = 0.0;
+    double v[1] = {0.0};
+    for (int c = c0 + threadIdx.x; c < c1; c += kThreads) {
+        const double b = mux[a.fidx[c]];
+        a.vx[c] = b;
+        a.vpx[c] = a.px[c] = a.d1x[c] = a.d2x[c] = a.sx[c] = 0.0;
         v[0] += b * b;
-        v[1] += f ? 1.0 : 0.0;
     }
-    for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
-        const bool d = a.cy[i] != 0;
-        const double b = d ? muy[i] : 0.0;
-        a.vy[i] = b;
-        a.vpy[i] = a.py[i] = a.d1y[i] = a.d2y[i] = a.sy[i] = 0.0;
+    for (int r = r0 + threadIdx.x; r < r1; r += kThreads) {
+        const double b = muy[a.didx[r]];
+        a.vy[r] = b;
+        a.vpy[r] = a.py[r] = a.d1y[r] = a.d2y[r] = a.sy[r] = 0.0;
         v[0] += b * b;
-        v[2] += d ? 1.0 : 0.0;
     }
-    block_sum<3>(v, red);
+    block_sum<1>(v, red);
     if (threadIdx.x == 0) {
         MrState s;
         memset(&s, 0, sizeof(s));
@@ -265,8 +266,8 @@ __global__ void __launch_bounds__(kThreads) k_mr_init(const __grid_constant__ Mr
         s.cs = -1.0;
         s.phibar = s.beta1;
         s.tol = tol;
-        s.free_cols = static_cast<int>(v[1]);
-        s.active_rows = static_cast<int>(v[2]);
+        s.free_cols = c1 - c0;
+        s.active_rows = r1 - r0;
         // In exact arithmetic MINRES ends within dim = |F| + |D| steps; finite
         // precision Lanczos needs a few times that on consistent systems, and an
         // inconsistent one (a wrong active set) never converges.
@@ -282,18 +283,14 @@ __global__ void __launch_bounds__(kThreads) k_mr_init(const __grid_constant__ Mr
     for (int i = r0 + threadIdx.x; i < r1; i += kThreads) a.vy[i] *= iv;
 }
 
-// p = K v with K = [[0, B^T], [B, 0]] in the full index space (zero outside the masks).
+// p = K v with K = [[0, B^T], [B, 0]] in the compact index space: the B pass
+// (rows D) gives the y-part, the B^T pass (rows F) the x-part.
 struct MrEpi {
-    const i8* __restrict__ code;
     double* __restrict__ out;
     const MrState* __restrict__ st;
-    int cols;
     __device__ __forceinline__ bool begin(int inst) const { return st[inst].done == 0; }
     __device__ __forceinline__ NoPre prefetch(int) const { return {}; }
-    __device__ __forceinline__ void operator()(int r, const double (&s)[1], const NoPre&) {
-        const int c = code[r];
-        out[r] = (cols ? c == 1 : c != 0) ? s[0] : 0.0;
-    }
+    __device__ __forceinline__ void operator()(int r, const double (&s)[1], const NoPre&) { out[r] = s[0]; }
 };
 struct MrOpArgs {
     CsrView<double> A, AT;
@@ -302,10 +299,10 @@ struct MrOpArgs {
 __global__ void __launch_bounds__(kThreads) k_mr_op(const __grid_constant__ MrOpArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (static_cast<int>(blockIdx.x) < a.A.nb) {
-        MrEpi e{a.v.cy, a.v.py, a.v.st, 0};
+        MrEpi e{a.v.py, a.v.st};
         spmv_run<1, double, double>(a.A, blockIdx.x, GatherOne<double>{a.v.vx}, e, smem);
     } else {
-        MrEpi e{a.v.cx, a.v.px, a.v.st, 1};
+        MrEpi e{a.v.px, a.v.st};
         spmv_run<1, double, double>(a.AT, blockIdx.x - a.A.nb, GatherOne<double>{a.v.vy}, e, smem);
     }
 }
@@ -409,6 +406,92 @@ __global__ void __launch_bounds__(kThreads) k_code_counts(const int* __restrict_
         }
         out[k] = make_int2(tf, td);
     }
+}
+
+// ---- the reduced system B = A'[D, F] in compact form, built per MINRES solve
+// (F: free columns, cx == 1; D: dual-active rows, cy != 0).  Flags with one
+// trailing 0, so that the exclusive scan's last entry is the count.
+__global__ void k_mr_flags(int n, int m, const i8* __restrict__ cx, const i8* __restrict__ cy, int* __restrict__ ff,
+                           int* __restrict__ df) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j <= n; j += stride) ff[j] = (j < n && cx[j] == 1) ? 1 : 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= m; i += stride) df[i] = (i < m && cy[i] != 0) ? 1 : 0;
+}
+
+// From the scanned flags: full -> compact maps (-1 outside F / D), compact ->
+// full lists, and each instance's compact offsets.
+__global__ void k_mr_maps(int n, int m, int count, const int* __restrict__ col_off, const int* __restrict__ row_off,
+                          const int* __restrict__ ff, const int* __restrict__ fs, const int* __restrict__ df,
+                          const int* __restrict__ ds, int* __restrict__ cmap, int* __restrict__ rmap,
+                          int* __restrict__ fidx, int* __restrict__ didx, int* __restrict__ f_off,
+                          int* __restrict__ d_off) {
+    const int stride = gridDim.x * blockDim.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int j = t; j < n; j += stride) {
+        cmap[j] = ff[j] ? fs[j] : -1;
+        if (ff[j]) fidx[fs[j]] = j;
+    }
+    for (int i = t; i < m; i += stride) {
+        rmap[i] = df[i] ? ds[i] : -1;
+        if (df[i]) didx[ds[i]] = i;
+    }
+    for (int k = t; k <= count; k += stride) {
+        f_off[k] = fs[col_off[k]];
+        d_off[k] = ds[row_off[k]];
+    }
+}
+
+// Entries of compact row r (full row rows[r] of ptr/idx) whose column maps
+// into the compact space: one warp per row.
+__global__ void k_mr_row_counts(int nr, const int* __restrict__ rows, const int* __restrict__ ptr,
+                                const int* __restrict__ idx, const int* __restrict__ map, int* __restrict__ cnt) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nr; r += nw) {
+        const int i = rows[r];
+        int c = 0;
+        for (int p = ptr[i] + lane; p < ptr[i + 1]; p += 32) c += map[idx[p]] >= 0;
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+        if (lane == 0) cnt[r] = c;
+    }
+}
+
+// The same entries, in source order, into out_ptr's slots, columns mapped:
+// each warp keeps its row's order with a ballot prefix.
+__global__ void k_mr_row_fill(int nr, const int* __restrict__ rows, const int* __restrict__ ptr,
+                              const int* __restrict__ idx, const double* __restrict__ val,
+                              const int* __restrict__ map, const int* __restrict__ out_ptr, int* __restrict__ out_idx,
+                              double* __restrict__ out_val) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nr; r += nw) {
+        const int i = rows[r];
+        int q = out_ptr[r];
+        for (int p0 = ptr[i]; p0 < ptr[i + 1]; p0 += 32) {
+            const int p = p0 + lane;
+            const int c = p < ptr[i + 1] ? map[idx[p]] : -1;
+            const unsigned keep = __ballot_sync(0xffffffffu, c >= 0);
+            if (c >= 0) {
+                const int at = q + __popc(keep & ((1u << lane) - 1u));
+                out_idx[at] = c;
+                out_val[at] = val[p];
+            }
+            q += __popc(keep);
+        }
+    }
+}
+
+// Compact solution -> full index space (zero outside F / D), for the
+// instances selected (sel == nullptr: all).
+__global__ void k_mr_scatter(int n, int m, const int* inst_col, const int* inst_row, const int* __restrict__ sel,
+                             const int* __restrict__ cmap, const int* __restrict__ rmap,
+                             const double* __restrict__ sx, const double* __restrict__ sy, double* __restrict__ ox,
+                             double* __restrict__ oy) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride)
+        if (sel == nullptr || sel[inst_of(inst_col, j)]) ox[j] = cmap[j] >= 0 ? sx[cmap[j]] : 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride)
+        if (sel == nullptr || sel[inst_of(inst_row, i)]) oy[i] = rmap[i] >= 0 ? sy[rmap[i]] : 0.0;
 }
 
 // Condition of the MINRES loop graph: repeat while some instance has not finished.
@@ -554,7 +637,15 @@ struct Diff {
     DevBuf<i8> scx, scy;            // projection codes of one segment: R n, R m
     int seg_valid = -1;             // segment whose iterates the buffers hold
     DevBuf<double> lx, ly, lq, lg, gc, glo, ghi, ga;
-    DevBuf<double> mr[12];
+    DevBuf<double> mr[12];          // MINRES vectors, compact index space (x-parts n, y-parts m long)
+    DevBuf<double> mr_sol_x, mr_sol_y;  // its solution in the full index space
+    // the reduced system of the last solve: flags and scans (n + 1, m + 1),
+    // maps, lists, per-instance compact offsets, B and B^T in CSR with schedules
+    DevBuf<int> mr_ff, mr_fs, mr_df, mr_ds, mr_cmap, mr_rmap, mr_fidx, mr_didx, mr_foff, mr_doff, mr_scan;
+    DevBuf<int> b_ptr, b_idx, bt_ptr, bt_idx;
+    DevBuf<double> b_val, bt_val;
+    DevSchedule b_s, bt_s;
+    std::vector<int> mr_foff_h, mr_doff_h, b_ptr_h, bt_ptr_h;
     DevBuf<MrState> mst;
     MrState* mst_host = nullptr;
     DevBuf<int> flags;              // per-instance selection (polish use / restore)
@@ -589,10 +680,10 @@ struct Diff {
 
     MrVecs mr_vecs() {
         MrVecs v;
-        v.col_off = P->d_col_off.get();
-        v.row_off = P->d_row_off.get();
-        v.cx = cx_at(0);
-        v.cy = cy_at(0);
+        v.col_off = mr_foff.get();
+        v.row_off = mr_doff.get();
+        v.fidx = mr_fidx.get();
+        v.didx = mr_didx.get();
         v.vx = mr[0].get(); v.vy = mr[1].get(); v.vpx = mr[2].get(); v.vpy = mr[3].get();
         v.px = mr[4].get(); v.py = mr[5].get(); v.d1x = mr[6].get(); v.d1y = mr[7].get();
         v.d2x = mr[8].get(); v.d2y = mr[9].get(); v.sx = mr[10].get(); v.sy = mr[11].get();
@@ -626,20 +717,86 @@ struct Diff {
         seg_valid = seg;
     }
 
+    // The reduced system of the codes of step 0 of the resident segment: F
+    // (free columns) and D (dual-active rows) of every instance, B = A'[D, F]
+    // and B^T = A'^T[F, D] in CSR over compact indices (entries in source
+    // order), and their row-block schedules, segmented by instance.
+    void build_reduced() {
+        Problem& p = *P;
+        cudaStream_t s = p.stream;
+        const int n = p.n, m = p.m, K = p.count;
+        const int gv = elem_grid(std::max(n, m) + 1, p.sms);
+        k_mr_flags<<<gv, kThreads, 0, s>>>(n, m, cx_at(0), cy_at(0), mr_ff.get(), mr_df.get());
+        exclusive_scan(mr_ff.get(), mr_fs.get(), n + 1, mr_scan.get(), s);
+        exclusive_scan(mr_df.get(), mr_ds.get(), m + 1, mr_scan.get(), s);
+        k_mr_maps<<<gv, kThreads, 0, s>>>(n, m, K, p.d_col_off.get(), p.d_row_off.get(), mr_ff.get(), mr_fs.get(),
+                                          mr_df.get(), mr_ds.get(), mr_cmap.get(), mr_rmap.get(), mr_fidx.get(),
+                                          mr_didx.get(), mr_foff.get(), mr_doff.get());
+        mr_foff_h.resize(K + 1);
+        mr_doff_h.resize(K + 1);
+        GB_CUDA(cudaMemcpyAsync(mr_foff_h.data(), mr_foff.get(), sizeof(int) * (K + 1), cudaMemcpyDeviceToHost, s));
+        GB_CUDA(cudaMemcpyAsync(mr_doff_h.data(), mr_doff.get(), sizeof(int) * (K + 1), cudaMemcpyDeviceToHost, s));
+        GB_CUDA(cudaStreamSynchronize(s));
+        const int nf = mr_foff_h[K], nd = mr_doff_h[K];
+        const int gw = elem_grid(static_cast<long long>(std::max(std::max(nf, nd), 1)) * 32, p.sms);
+        GB_CUDA(cudaMemsetAsync(b_ptr.get() + nd, 0, sizeof(int), s));
+        GB_CUDA(cudaMemsetAsync(bt_ptr.get() + nf, 0, sizeof(int), s));
+        if (nd) k_mr_row_counts<<<gw, kThreads, 0, s>>>(nd, mr_didx.get(), p.A.ptr.get(), p.A.idx.get(),
+                                                        mr_cmap.get(), b_ptr.get());
+        if (nf) k_mr_row_counts<<<gw, kThreads, 0, s>>>(nf, mr_fidx.get(), p.AT.ptr.get(), p.AT.idx.get(),
+                                                        mr_rmap.get(), bt_ptr.get());
+        exclusive_scan(b_ptr.get(), b_ptr.get(), nd + 1, mr_scan.get(), s);
+        exclusive_scan(bt_ptr.get(), bt_ptr.get(), nf + 1, mr_scan.get(), s);
+        if (nd) k_mr_row_fill<<<gw, kThreads, 0, s>>>(nd, mr_didx.get(), p.A.ptr.get(), p.A.idx.get(),
+                                                      p.A.val64.get(), mr_cmap.get(), b_ptr.get(), b_idx.get(),
+                                                      b_val.get());
+        if (nf) k_mr_row_fill<<<gw, kThreads, 0, s>>>(nf, mr_fidx.get(), p.AT.ptr.get(), p.AT.idx.get(),
+                                                      p.AT.val64.get(), mr_rmap.get(), bt_ptr.get(), bt_idx.get(),
+                                                      bt_val.get());
+        b_ptr_h.resize(nd + 1);
+        bt_ptr_h.resize(nf + 1);
+        GB_CUDA(cudaMemcpyAsync(b_ptr_h.data(), b_ptr.get(), sizeof(int) * (nd + 1), cudaMemcpyDeviceToHost, s));
+        GB_CUDA(cudaMemcpyAsync(bt_ptr_h.data(), bt_ptr.get(), sizeof(int) * (nf + 1), cudaMemcpyDeviceToHost, s));
+        GB_CUDA(cudaStreamSynchronize(s));
+        b_s.upload(build_schedule(b_ptr_h.data(), nd, mr_doff_h.data(), K), 1, s);
+        bt_s.upload(build_schedule(bt_ptr_h.data(), nf, mr_foff_h.data(), K), 1, s);
+        launches += 10;
+    }
+    CsrView<double> reduced_view(const DevBuf<int>& ptr, const DevBuf<int>& idx, const DevBuf<double>& val,
+                                 const DevSchedule& sc, int rows) const {
+        CsrView<double> v;
+        v.ptr = ptr.get();
+        v.idx = idx.get();
+        v.val = val.get();
+        v.blocks = sc.blocks.get();
+        v.slots = sc.slots.get();
+        v.counters = sc.counters.get();
+        v.bits = sc.bits.get();
+        v.rows = rows;
+        v.nb = sc.nb;
+        v.vec = 1;  // idx / val allocated with padded_nnz
+        v.nc = kLoadPlain;
+        return v;
+    }
+
     // Per-instance MINRES on K = [[0, B^T], [B, 0]] with B = A'[D, F] read from
-    // the codes of step 0 of the resident segment; solution in mr[10], mr[11];
-    // per-instance state left in mst_host.
+    // the codes of step 0 of the resident segment, in the compact index space
+    // of (F, D); the solution goes to mr_sol_x / mr_sol_y in the full index
+    // space (zero outside F / D); per-instance state left in mst_host.
     // sel (device, may be NULL): only the instances with sel[k] != 0 start a
-    // new solve; the others keep their state and solution.
+    // new solve; the others keep their state and full-space solution.
     void minres(const double* rhs_x, const double* rhs_y, const int* sel = nullptr) {
         Problem& p = *P;
         cudaStream_t s = p.stream;
         const size_t smem = spmv_smem_bytes<1, double>();
+        build_reduced();
         MrVecs v = mr_vecs();
         k_mr_init<<<p.count, kThreads, 0, s>>>(v, rhs_x, rhs_y, mr_max, mr_tol, sel);
         launches += 1;
-        MrOpArgs oa{p.A.view<double>(), p.AT.view<double>(), v};
+        const int nd = mr_doff_h[p.count], nf = mr_foff_h[p.count];
+        MrOpArgs oa{reduced_view(b_ptr, b_idx, b_val, b_s, nd), reduced_view(bt_ptr, bt_idx, bt_val, bt_s, nf), v};
         const int nb = oa.A.nb + oa.AT.nb;
+        mr_graph.reset();  // it holds the previous system's schedules
         // The steps run as one CUDA graph: a conditional while node whose body is
         // kMrChunk steps and a test of the per-instance "done" flags, so the
         // loop needs no host round trip.  Every instance stops at its own step
@@ -677,11 +834,14 @@ struct Diff {
             mr_graph = std::move(g);
         }
         GB_CUDA(cudaGraphLaunch(mr_graph->exec, s));
+        k_mr_scatter<<<elem_grid(std::max(p.n, p.m), p.sms), kThreads, 0, s>>>(
+            p.n, p.m, p.icol(), p.irow(), sel, mr_cmap.get(), mr_rmap.get(), mr[10].get(), mr[11].get(),
+            mr_sol_x.get(), mr_sol_y.get());
         GB_CUDA(cudaMemcpyAsync(mst_host, mst.get(), sizeof(MrState) * p.count, cudaMemcpyDeviceToHost, s));
         GB_CUDA(cudaStreamSynchronize(s));
         long long steps = 0;
         for (int k = 0; k < p.count; ++k) steps = std::max<long long>(steps, mst_host[k].it);
-        launches += ((steps + kMrChunk - 1) / kMrChunk) * (2 * kMrChunk + 1);
+        launches += 1 + ((steps + kMrChunk - 1) / kMrChunk) * (2 * kMrChunk + 1);
     }
 };
 
@@ -702,6 +862,21 @@ void diff_alloc(Diff& D) {
     D.ga.reset(z);
     D.io_z.reset(z);
     for (int k = 0; k < 12; ++k) D.mr[k].reset(k % 2 == 0 ? n : m);
+    D.mr_sol_x.reset(n);
+    D.mr_sol_y.reset(m);
+    for (DevBuf<int>* b : {&D.mr_ff, &D.mr_fs}) b->reset(n + 1);
+    for (DevBuf<int>* b : {&D.mr_df, &D.mr_ds}) b->reset(m + 1);
+    for (DevBuf<int>* b : {&D.mr_cmap, &D.mr_fidx}) b->reset(n);
+    for (DevBuf<int>* b : {&D.mr_rmap, &D.mr_didx}) b->reset(m);
+    D.mr_foff.reset(P.count + 1);
+    D.mr_doff.reset(P.count + 1);
+    D.mr_scan.reset(std::max(scan_tiles(n + 1), scan_tiles(m + 1)));
+    D.b_ptr.reset(m + 1);
+    D.bt_ptr.reset(n + 1);
+    D.b_idx.reset(padded_nnz(z));  // B and B^T hold at most A's nonzeros
+    D.bt_idx.reset(padded_nnz(z));
+    D.b_val.reset(padded_nnz(z));
+    D.bt_val.reset(padded_nnz(z));
     D.mst.reset(P.count);
     D.flags.reset(P.count);
     D.mst_host = static_cast<MrState*>(host_alloc(sizeof(MrState) * P.count));
@@ -835,7 +1010,7 @@ void polish(Diff& D, double accept_tol, const std::vector<int>& todo) {
     }
     D.flags.upload(D.flags_host, P.count, s);
     k_polish_point<<<gv, kThreads, 0, s>>>(n, m, P.icol(), P.irow(), D.flags.get(), D.cx_at(0), D.cy_at(0),
-                                          D.mr[10].get(), D.mr[11].get(), P.l.get(), P.u.get(), P.x64.get(),
+                                          D.mr_sol_x.get(), D.mr_sol_y.get(), P.l.get(), P.u.get(), P.x64.get(),
                                           P.y64.get());
     certify(P);
     bool any_restore = false;
@@ -1056,7 +1231,7 @@ void diff_backward(Diff& D, const double* dl_dx, const double* dl_dy, double* dl
     if (D.mr_max > 0) {
         D.minres(D.lx.get(), D.ly.get());
         k_implicit_grads<<<gall, kThreads, 0, s>>>(n, m, nnz, P.row_of.get(), P.A.idx.get(), D.cy_at(0),
-                                                   D.mr[10].get(), D.mr[11].get(), D.xb_at(0), D.y_at(0),
+                                                   D.mr_sol_x.get(), D.mr_sol_y.get(), D.xb_at(0), D.y_at(0),
                                                    D.gc.get(), D.glo.get(), D.ghi.get(), D.ga.get());
         D.launches += 1;
         for (int k = 0; k < P.count; ++k) {
