@@ -797,43 +797,57 @@ struct Diff {
         MrOpArgs oa{reduced_view(b_ptr, b_idx, b_val, b_s, nd), reduced_view(bt_ptr, bt_idx, bt_val, bt_s, nf), v};
         const int nb = oa.A.nb + oa.AT.nb;
         mr_graph.reset();  // it holds the previous system's schedules
-        // The steps run as one CUDA graph: a conditional while node whose body is
-        // kMrChunk steps and a test of the per-instance "done" flags, so the
-        // loop needs no host round trip.  Every instance stops at its own step
-        // bound (MrState::max_it), so the loop ends.
-        if (!mr_graph) {
-            auto g = std::make_unique<LevelGraph>();
-            GB_CUDA(cudaGraphCreate(&g->graph, 0));
-            cudaGraphConditionalHandle h;
-            GB_CUDA(cudaGraphConditionalHandleCreate(&h, g->graph, 1, cudaGraphCondAssignDefault));
-            cudaGraphNodeParams cp = {};
-            cp.type = cudaGraphNodeTypeConditional;
-            cp.conditional.handle = h;
-            cp.conditional.type = cudaGraphCondTypeWhile;
-            cp.conditional.size = 1;
-            cudaGraphNode_t node;
-            GB_CUDA(cudaGraphAddNode(&node, g->graph, nullptr, 0, &cp));
-            cudaGraph_t body = cp.conditional.phGraph_out[0];
-            cudaStream_t cs;
-            GB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-            GB_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-            for (int c = 0; c < kMrChunk; ++c) {
-                if (nb) k_mr_op<<<nb, kThreads, smem, cs>>>(oa);
-                k_mr_update<<<p.count, kThreads, 0, cs>>>(v);
+        if (host_loop_mode()) {  // the same steps from the host, one state read-back per chunk
+            for (;;) {
+                for (int c = 0; c < kMrChunk; ++c) {
+                    if (nb) k_mr_op<<<nb, kThreads, smem, s>>>(oa);
+                    k_mr_update<<<p.count, kThreads, 0, s>>>(v);
+                }
+                GB_CUDA(cudaMemcpyAsync(mst_host, mst.get(), sizeof(MrState) * p.count, cudaMemcpyDeviceToHost, s));
+                GB_CUDA(cudaStreamSynchronize(s));
+                bool any = false;
+                for (int k = 0; k < p.count; ++k) any |= mst_host[k].done == 0;
+                if (!any) break;
             }
-            k_mr_cond<<<1, kThreads, 0, cs>>>(mst.get(), p.count, static_cast<unsigned long long>(h));
-            const cudaError_t e = cudaGetLastError();
-            cudaGraph_t done_body = nullptr;
-            const cudaError_t e2 = cudaStreamEndCapture(cs, &done_body);
-            cudaStreamDestroy(cs);
-            if (e != cudaSuccess || e2 != cudaSuccess) {
-                g->graph = nullptr;  // a failed capture: leak the half-built graph rather than destroy it
-                GB_CUDA(e != cudaSuccess ? e : e2);
+        } else {
+            // The steps run as one CUDA graph: a conditional while node whose body is
+            // kMrChunk steps and a test of the per-instance "done" flags, so the
+            // loop needs no host round trip.  Every instance stops at its own step
+            // bound (MrState::max_it), so the loop ends.
+            if (!mr_graph) {
+                auto g = std::make_unique<LevelGraph>();
+                GB_CUDA(cudaGraphCreate(&g->graph, 0));
+                cudaGraphConditionalHandle h;
+                GB_CUDA(cudaGraphConditionalHandleCreate(&h, g->graph, 1, cudaGraphCondAssignDefault));
+                cudaGraphNodeParams cp = {};
+                cp.type = cudaGraphNodeTypeConditional;
+                cp.conditional.handle = h;
+                cp.conditional.type = cudaGraphCondTypeWhile;
+                cp.conditional.size = 1;
+                cudaGraphNode_t node;
+                GB_CUDA(cudaGraphAddNode(&node, g->graph, nullptr, 0, &cp));
+                cudaGraph_t body = cp.conditional.phGraph_out[0];
+                cudaStream_t cs;
+                GB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+                GB_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+                for (int c = 0; c < kMrChunk; ++c) {
+                    if (nb) k_mr_op<<<nb, kThreads, smem, cs>>>(oa);
+                    k_mr_update<<<p.count, kThreads, 0, cs>>>(v);
+                }
+                k_mr_cond<<<1, kThreads, 0, cs>>>(mst.get(), p.count, static_cast<unsigned long long>(h));
+                const cudaError_t e = cudaGetLastError();
+                cudaGraph_t done_body = nullptr;
+                const cudaError_t e2 = cudaStreamEndCapture(cs, &done_body);
+                cudaStreamDestroy(cs);
+                if (e != cudaSuccess || e2 != cudaSuccess) {
+                    g->graph = nullptr;  // a failed capture: leak the half-built graph rather than destroy it
+                    GB_CUDA(e != cudaSuccess ? e : e2);
+                }
+                GB_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
+                mr_graph = std::move(g);
             }
-            GB_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
-            mr_graph = std::move(g);
+            GB_CUDA(cudaGraphLaunch(mr_graph->exec, s));
         }
-        GB_CUDA(cudaGraphLaunch(mr_graph->exec, s));
         k_mr_scatter<<<elem_grid(std::max(p.n, p.m), p.sms), kThreads, 0, s>>>(
             p.n, p.m, p.icol(), p.irow(), sel, mr_cmap.get(), mr_rmap.get(), mr[10].get(), mr[11].get(),
             mr_sol_x.get(), mr_sol_y.get());
@@ -878,6 +892,13 @@ void diff_alloc(Diff& D) {
     D.b_val.reset(padded_nnz(z));
     D.bt_val.reset(padded_nnz(z));
     D.mst.reset(P.count);
+    {  // an instance no solve has selected yet counts as finished
+        std::vector<MrState> idle(P.count);
+        std::memset(idle.data(), 0, sizeof(MrState) * idle.size());
+        for (MrState& st : idle) st.done = 1;
+        D.mst.upload(idle.data(), idle.size(), P.stream);
+        GB_CUDA(cudaStreamSynchronize(P.stream));
+    }
     D.flags.reset(P.count);
     D.mst_host = static_cast<MrState*>(host_alloc(sizeof(MrState) * P.count));
     D.flags_host = static_cast<int*>(host_alloc(sizeof(int) * P.count));

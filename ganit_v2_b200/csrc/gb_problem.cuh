@@ -173,6 +173,9 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt);
 void solve_problem(Problem& P, const gb_options* opt, gb_result* res);
 void set_start(Problem& P, int inst, const double* x, const double* y);
 void clear_start(Problem& P);
+// GANIT_B200_LAUNCH=stream: loops that otherwise run as conditional CUDA
+// graphs are driven from the host (kernel profilers see their kernels).
+bool host_loop_mode();
 void certify(Problem& P);  // FP64 KKT of (x64, y64) of every instance into st_host[k].kcert
 
 // Runs f, turning exceptions into the ABI's status codes (message in g_last_error).
