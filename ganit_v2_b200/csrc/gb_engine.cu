@@ -672,6 +672,24 @@ void launch_iteration(Problem& P, VecSet<V>& vs, int k, cudaStream_t s, long lon
     nl += 2;
 }
 
+// k_decide, preceded for a single problem with more than kDecideWide row
+// blocks by k_terms (its term sums, one CTA per term; same bits).  Returns
+// the launches.
+template <class M, class V>
+int launch_decide(Problem& P, EvalArgs<M, V>& ea, cudaStream_t s, bool pdl) {
+    int nl = 1;
+    ea.terms_ready = 0;
+    if (P.count == 1 && ea.A.nb + ea.AT.nb > kDecideWide) {
+        ea.terms_ready = 1;
+        if (pdl) launch_pdl(k_terms<M, V>, kTerms, kThreads, 0, s, ea);
+        else k_terms<M, V><<<kTerms, kThreads, 0, s>>>(ea);
+        nl += 1;
+    }
+    if (pdl) launch_pdl(k_decide<M, V>, decide_grid(P.count), kThreads, 0, s, ea);
+    else k_decide<M, V><<<decide_grid(P.count), kThreads, 0, s>>>(ea);
+    return nl;
+}
+
 // Body of the phase loop: check_every iterations, KKT check, restart.
 // use_cond = 0 when the body is launched from the host loop instead of the graph.
 template <class M, class V>
@@ -691,11 +709,11 @@ long long capture_body(Problem& P, int ce, cudaGraphConditionalHandle cond, cuda
         launch_pdl(k_eval<M, V, 3, 3>, grid, kThreads, spmv_smem_bytes<3, V>(), s, ea);
     else
         launch_pdl(k_eval<M, V, 2, 3>, grid, kThreads, spmv_smem_bytes<3, V>(), s, ea);
-    launch_pdl(k_decide<M, V>, decide_grid(P.count), kThreads, 0, s, ea);
+    nl += launch_decide<M, V>(P, ea, s, true);
     RestartArgs<V> ra{xc, yc, vs.x0.get(), vs.y0.get(), vs.xr.get(), vs.yr.get(), vs.sumx.get(), vs.sumy.get(),
                       P.n, P.m, P.icol(), P.irow(), P.st.get()};
     launch_pdl(k_restart<V>, elem_grid(std::max(P.n, P.m), P.sms), kThreads, 0, s, ra);
-    nl += 3;
+    nl += 2;
     return nl;
 }
 
@@ -900,8 +918,7 @@ void run_phase(Problem& P, const gb_options* opt, double tol, int stall_exit, in
     if (P.has_q) launch_qx<M, V>(P, vs, vs.x0.get(), vs.qx.get(), s, P.launches);
     EvalArgs<M, V> ea = eval_args<M, V>(P, vs, vs.x0.get(), vs.y0.get(), kEvalInit, P.has_q);
     k_eval<M, V, 1, 1><<<ea.A.nb + ea.AT.nb, kThreads, spmv_smem_bytes<1, V>(), s>>>(ea);
-    k_decide<M, V><<<decide_grid(P.count), kThreads, 0, s>>>(ea);
-    P.launches += 2;
+    P.launches += 1 + launch_decide<M, V>(P, ea, s, false);
     long long per_body = 0;
     long long bodies = 0;
     if (host_loop_mode()) {
@@ -944,8 +961,7 @@ void certify(Problem& P) {
     if (P.has_q) launch_qx<double, double>(P, vs, P.x64.get(), vs.qx.get(), s, P.launches);
     EvalArgs<double, double> ea = eval_args<double, double>(P, vs, P.x64.get(), P.y64.get(), kEvalCertify, P.has_q);
     k_eval<double, double, 1, 1><<<ea.A.nb + ea.AT.nb, kThreads, spmv_smem_bytes<1, double>(), s>>>(ea);
-    k_decide<double, double><<<decide_grid(P.count), kThreads, 0, s>>>(ea);
-    P.launches += 2;
+    P.launches += 1 + launch_decide<double, double>(P, ea, s, false);
     sync_state(P);
 }
 

@@ -252,11 +252,13 @@ struct EvalArgs {
     unsigned long long cond;     // cudaGraphConditionalHandle of the phase loop
     int use_cond;                // 1 inside the loop body: the decision drives the loop
     unsigned* sync = nullptr;    // k_decide over several CTAs: {arrivals, any instance active}
+    int terms_ready = 0;         // single instance: k_terms summed its terms into inst_terms
 };
 
 // k_decide's grid: one CTA for a single problem, else one CTA per
 // kDecideInst instances (one instance per warp while reducing).
 constexpr int kDecideInst = kWarps;
+constexpr int kDecideWide = 128;  // blocks above which an instance's terms are summed by a whole CTA
 inline int decide_grid(int count) { return count == 1 ? 1 : (count + kDecideInst - 1) / kDecideInst; }
 
 template <class V>
@@ -553,6 +555,25 @@ __global__ void __launch_bounds__(kThreads) k_eval(const __grid_constant__ EvalA
 // instance per warp).  With several CTAs the last to arrive sets the phase
 // loop's condition from the OR of every CTA's "some instance still active" and
 // re-arms the two sync words.
+// The term sums of a single instance with more than kDecideWide blocks,
+// one CTA per term, before k_decide: CTA q folds term q over the instance's
+// blocks exactly as k_decide's whole-CTA path does (thread t takes blocks
+// t, t + kThreads, ..., then block_sum), so the sums are the same bits, and
+// the 22 folds run side by side instead of in one CTA.
+template <class M, class V>
+__global__ void __launch_bounds__(kThreads) k_terms(const __grid_constant__ EvalArgs<M, V> a) {
+    pdl_enter();
+    __shared__ double red[kWarps];
+    const int q = blockIdx.x;
+    const size_t nb = static_cast<size_t>(a.A.nb + a.AT.nb);
+    const int b0 = q < kRowTerms ? a.seg_a[0] : a.A.nb + a.seg_t[0];
+    const int b1 = q < kRowTerms ? a.seg_a[1] : a.A.nb + a.seg_t[1];
+    double v[1] = {0.0};
+    for (int b = b0 + static_cast<int>(threadIdx.x); b < b1; b += kThreads) v[0] += __ldcg(a.partials + q * nb + b);
+    block_sum<1>(v, red);
+    if (threadIdx.x == 0) a.inst_terms[q] = v[0];
+}
+
 template <class M, class V>
 __global__ void __launch_bounds__(kThreads) k_decide(const __grid_constant__ EvalArgs<M, V> a) {
     pdl_enter();
@@ -581,7 +602,7 @@ __global__ void __launch_bounds__(kThreads) k_decide(const __grid_constant__ Eva
         decide(s, T, a.mode);
         any_active |= s.active;
     };
-    constexpr int kWide = 128;  // blocks above which an instance gets the whole CTA
+    constexpr int kWide = kDecideWide;
     for (int k = k0; k < k1; ++k) {
         const int nblk = (a.seg_a[k + 1] - a.seg_a[k]) + (a.seg_t[k + 1] - a.seg_t[k]);
         if (nblk <= kWide) continue;
@@ -591,9 +612,17 @@ __global__ void __launch_bounds__(kThreads) k_decide(const __grid_constant__ Eva
             continue;
         }
         double T[kTerms];
-        load_terms(k, threadIdx.x, kThreads, T);
-        block_sum<kTerms>(T, red);
-        if (threadIdx.x == 0) finish(s, T);
+        if (a.terms_ready) {  // k_terms folded them already, in this same order
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int q = 0; q < kTerms; ++q) T[q] = __ldcg(a.inst_terms + static_cast<size_t>(k) * kTerms + q);
+                finish(s, T);
+            }
+        } else {
+            load_terms(k, threadIdx.x, kThreads, T);
+            block_sum<kTerms>(T, red);
+            if (threadIdx.x == 0) finish(s, T);
+        }
         __syncthreads();
     }
     for (int k = k0 + wid; k < k1; k += kWarps) {
