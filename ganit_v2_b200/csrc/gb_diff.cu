@@ -1124,11 +1124,18 @@ void diff_forward(Diff& D, const gb_options* opt, gb_result* res, double* x_out,
         launches += 1;
         if (left == 0) break;
         // the next round starts every instance from its current point (original units)
+        // and primal weight
         k_unscale<<<gv, kThreads, 0, s>>>(P.n, P.m, P.icol(), P.irow(), P.x64.get(), P.y64.get(), P.C.get(),
                                          P.R.get(), P.scal.get(), P.xo.get(), P.yo.get());
         if (!P.x_start.get()) {
             P.x_start.reset(std::max(P.n, 1));
             P.y_start.reset(std::max(P.m, 1));
+        }
+        {  // and with its final primal weight, not the cold default
+            std::vector<double> w(K);
+            for (int k = 0; k < K; ++k) w[k] = P.st_host[k].w;
+            P.w_start.reset(K);
+            P.w_start.upload(w.data(), K, s);
         }
         GB_CUDA(cudaMemcpyAsync(P.x_start.get(), P.xo.get(), D.n() * sizeof(double), cudaMemcpyDeviceToDevice, s));
         GB_CUDA(cudaMemcpyAsync(P.y_start.get(), P.yo.get(), D.m() * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -1139,6 +1146,7 @@ void diff_forward(Diff& D, const gb_options* opt, gb_result* res, double* x_out,
         P.x_start.release();
         P.y_start.release();
     }
+    P.w_start.release();
     if (any_kept) {  // vertices certified in an earlier round replace what later rounds left there
         for (int k = 0; k < K; ++k) D.flags_host[k] = kept[k];
         D.flags.upload(D.flags_host, K, s);

@@ -841,6 +841,12 @@ __global__ void k_init_state(int count, SolveState* st, const double* sc, int ha
     st[k] = s;
 }
 
+// Primal weight of a warm start (Problem::w_start, entries > 0), over k_init_state's w0.
+__global__ void k_set_w(int count, SolveState* st, const double* w) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count && w[k] > 0.0) st[k].w = w[k];
+}
+
 __global__ void k_activate_all(int count, SolveState* st) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < count) st[k].active = st[k].in_phase = 1;
@@ -999,6 +1005,10 @@ void solve_problem(Problem& P, const gb_options* opt, gb_result* res) {
             P.n, P.m, P.icol(), P.irow(), P.l.get(), P.u.get(), P.C.get(), P.R.get(), P.scal.get(),
             P.x_start.get(), P.y_start.get(), P.x64.get(), P.y64.get());
         P.launches += 1;
+        if (P.w_start.get()) {
+            k_set_w<<<div_up(K, kThreads), kThreads, 0, s>>>(K, P.st.get(), P.w_start.get());
+            P.launches += 1;
+        }
     }
     P.results.assign(K, InstanceResult{});
     std::vector<int> ex(K, kIterLimit), done(K, 0);

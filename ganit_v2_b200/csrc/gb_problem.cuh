@@ -138,6 +138,7 @@ struct Problem {
     // Phase graphs: levels <f32,f32>, <f32,f64>, <f64,f64>, <bf16,f32>, then the
     // same four for phases that run on block lists.
     std::unique_ptr<LevelGraph> graphs[8];
+    DevBuf<double> w_start;               // per-instance primal weight of a warm start (<= 0: the default)
     // Row blocks of the current phase when only some instances of a batch take
     // part and their blocks are at most half of all: copies of those
     // instances' RowBlocks, which the iteration kernels of level list_level
