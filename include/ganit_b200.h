@@ -455,8 +455,8 @@ int gb_strong_branch(const gb_lp* lp, const double* x, const double* y, int32_t 
  * inconsistent), the excess rows leave D smallest |y| first (equality rows
  * stay) or the excess free columns go to their nearest finite bound before
  * the solve (info.active_set_repaired).  With polishing on
- * (and implicit_max_iters > 0) and opt->tol below 1e-4, the solve goes in
- * rounds: first to 1e-4; every instance whose polished vertex certifies at
+ * (and implicit_max_iters > 0) and opt->tol below 4e-4, the solve goes in
+ * rounds: first to 4e-4; every instance whose polished vertex certifies at
  * opt->tol keeps it; the rest continue, warm-started from their points, at a
  * tolerance ten times tighter per round, down to opt->tol, where the last
  * round polishes as above (results[].iterations counts every round).
