@@ -409,13 +409,18 @@ __global__ void __launch_bounds__(kThreads) k_code_counts(const int* __restrict_
 }
 
 // ---- the reduced system B = A'[D, F] in compact form, built per MINRES solve
-// (F: free columns, cx == 1; D: dual-active rows, cy != 0).  Flags with one
-// trailing 0, so that the exclusive scan's last entry is the count.
-__global__ void k_mr_flags(int n, int m, const i8* __restrict__ cx, const i8* __restrict__ cy, int* __restrict__ ff,
+// (F: free columns, cx == 1; D: dual-active rows, cy != 0) of the instances
+// a solve selects (sel == nullptr: all), so that a solve for a few instances
+// launches their blocks alone.  Flags with one trailing 0, so that the
+// exclusive scan's last entry is the count.
+__global__ void k_mr_flags(int n, int m, const i8* __restrict__ cx, const i8* __restrict__ cy, const int* inst_col,
+                           const int* inst_row, const int* __restrict__ sel, int* __restrict__ ff,
                            int* __restrict__ df) {
     const int stride = gridDim.x * blockDim.x;
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j <= n; j += stride) ff[j] = (j < n && cx[j] == 1) ? 1 : 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= m; i += stride) df[i] = (i < m && cy[i] != 0) ? 1 : 0;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j <= n; j += stride)
+        ff[j] = (j < n && cx[j] == 1 && (sel == nullptr || sel[inst_of(inst_col, j)])) ? 1 : 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= m; i += stride)
+        df[i] = (i < m && cy[i] != 0 && (sel == nullptr || sel[inst_of(inst_row, i)])) ? 1 : 0;
 }
 
 // From the scanned flags: full -> compact maps (-1 outside F / D), compact ->
@@ -720,13 +725,15 @@ struct Diff {
     // The reduced system of the codes of step 0 of the resident segment: F
     // (free columns) and D (dual-active rows) of every instance, B = A'[D, F]
     // and B^T = A'^T[F, D] in CSR over compact indices (entries in source
-    // order), and their row-block schedules, segmented by instance.
-    void build_reduced() {
+    // order), and their row-block schedules, segmented by instance; only the
+    // instances `sel` selects (nullptr: all) get rows and columns.
+    void build_reduced(const int* sel) {
         Problem& p = *P;
         cudaStream_t s = p.stream;
         const int n = p.n, m = p.m, K = p.count;
         const int gv = elem_grid(std::max(n, m) + 1, p.sms);
-        k_mr_flags<<<gv, kThreads, 0, s>>>(n, m, cx_at(0), cy_at(0), mr_ff.get(), mr_df.get());
+        k_mr_flags<<<gv, kThreads, 0, s>>>(n, m, cx_at(0), cy_at(0), p.icol(), p.irow(), sel, mr_ff.get(),
+                                           mr_df.get());
         exclusive_scan(mr_ff.get(), mr_fs.get(), n + 1, mr_scan.get(), s);
         exclusive_scan(mr_df.get(), mr_ds.get(), m + 1, mr_scan.get(), s);
         k_mr_maps<<<gv, kThreads, 0, s>>>(n, m, K, p.d_col_off.get(), p.d_row_off.get(), mr_ff.get(), mr_fs.get(),
@@ -789,7 +796,7 @@ struct Diff {
         Problem& p = *P;
         cudaStream_t s = p.stream;
         const size_t smem = spmv_smem_bytes<1, double>();
-        build_reduced();
+        build_reduced(sel);
         MrVecs v = mr_vecs();
         k_mr_init<<<p.count, kThreads, 0, s>>>(v, rhs_x, rhs_y, mr_max, mr_tol, sel);
         launches += 1;
@@ -1232,6 +1239,7 @@ void diff_backward(Diff& D, const double* dl_dx, const double* dl_dy, double* dl
     GB_CUDA(cudaMemsetAsync(D.ga.get(), 0, D.ga.size() * sizeof(double), s));
     D.launches += 1;
 
+    StageTrace tr{s, "diff backward"};
     // 3. reverse through the tail, last segment first
     const size_t smem = spmv_smem_bytes<1, double>();
     const CsrView<double> A = P.A.view<double>(), AT = P.AT.view<double>();
@@ -1258,9 +1266,11 @@ void diff_backward(Diff& D, const double* dl_dx, const double* dl_dy, double* dl
     }
     // (lx, ly) now hold mu_0, the adjoint at the tail start; segment 0's step 0 is resident.
 
+    tr.mark("reverse pass");
     // 4. implicit completion
     if (D.mr_max > 0) {
         D.minres(D.lx.get(), D.ly.get());
+        tr.mark("completion");
         k_implicit_grads<<<gall, kThreads, 0, s>>>(n, m, nnz, P.row_of.get(), P.A.idx.get(), D.cy_at(0),
                                                    D.mr_sol_x.get(), D.mr_sol_y.get(), D.xb_at(0), D.y_at(0),
                                                    D.gc.get(), D.glo.get(), D.ghi.get(), D.ga.get());
