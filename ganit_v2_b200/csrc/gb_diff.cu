@@ -35,6 +35,8 @@
 //   5. Gradients go back through the scaling of src/scaling.cpp:75-101 with
 //      the scaling factors held constant.
 #include <algorithm>
+#include <cstdlib>
+#include <string>
 #include <cstring>
 #include <memory>
 
@@ -312,34 +314,46 @@ __global__ void __launch_bounds__(kThreads) k_mr_op(const __grid_constant__ MrOp
     }
 }
 
-// One MINRES step per instance (one CTA per instance; fixed-order reductions):
-// Lanczos (alpha, beta), the two Givens rotations, direction and solution update.
-__global__ void __launch_bounds__(kThreads) k_mr_update(const __grid_constant__ MrVecs a) {
-    __shared__ double red[kWarps];
-    __shared__ double bc[6];
-    const int k = blockIdx.x;
-    MrState* sp = a.st + k;
-    if (sp->done) return;
+// One MINRES step of instance k by its CTA (fixed-order reductions): Lanczos
+// (alpha, beta), the two Givens rotations, direction and solution update.
+// p = K v is in px / py on entry.
+// Sum of one value per thread over an NT-thread CTA into thread 0's v[0], in
+// the order of block_sum (each warp's shuffle sum, then the warps in order).
+template <int NT>
+__device__ __forceinline__ void mr_cta_sum(double (&v)[1], double* red) {
+    const double t = warp_sum(v[0]);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double u = 0.0;
+        for (int w = 0; w < NT / 32; ++w) u += red[w];
+        v[0] = u;
+    }
+    __syncthreads();
+}
+
+template <int NT>
+__device__ __forceinline__ void mr_update_step(const MrVecs& a, int k, MrState* sp, double* red, double* bc) {
     const int c0 = a.col_off[k], c1 = a.col_off[k + 1], r0 = a.row_off[k], r1 = a.row_off[k + 1];
     double v[1] = {0.0};
-    for (int j = c0 + threadIdx.x; j < c1; j += kThreads) v[0] += a.vx[j] * a.px[j];
-    for (int i = r0 + threadIdx.x; i < r1; i += kThreads) v[0] += a.vy[i] * a.py[i];
-    block_sum<1>(v, red);
+    for (int j = c0 + threadIdx.x; j < c1; j += NT) v[0] += a.vx[j] * a.px[j];
+    for (int i = r0 + threadIdx.x; i < r1; i += NT) v[0] += a.vy[i] * a.py[i];
+    mr_cta_sum<NT>(v, red);
     if (threadIdx.x == 0) bc[0] = v[0];
     __syncthreads();
     const double alpha = bc[0], beta = sp->beta;
     v[0] = 0.0;
-    for (int j = c0 + threadIdx.x; j < c1; j += kThreads) {
+    for (int j = c0 + threadIdx.x; j < c1; j += NT) {
         const double p = a.px[j] - alpha * a.vx[j] - beta * a.vpx[j];
         a.px[j] = p;
         v[0] += p * p;
     }
-    for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
+    for (int i = r0 + threadIdx.x; i < r1; i += NT) {
         const double p = a.py[i] - alpha * a.vy[i] - beta * a.vpy[i];
         a.py[i] = p;
         v[0] += p * p;
     }
-    block_sum<1>(v, red);
+    mr_cta_sum<NT>(v, red);
     if (threadIdx.x == 0) {
         MrState s = *sp;
         const double bn = sqrt(v[0]);
@@ -367,7 +381,7 @@ __global__ void __launch_bounds__(kThreads) k_mr_update(const __grid_constant__ 
     }
     __syncthreads();
     const double phi = bc[1], ig = bc[2], oldeps = bc[3], delta = bc[4], ib = bc[5];
-    for (int j = c0 + threadIdx.x; j < c1; j += kThreads) {
+    for (int j = c0 + threadIdx.x; j < c1; j += NT) {
         const double w = (a.vx[j] - oldeps * a.d2x[j] - delta * a.d1x[j]) * ig;
         a.d2x[j] = a.d1x[j];
         a.d1x[j] = w;
@@ -375,13 +389,70 @@ __global__ void __launch_bounds__(kThreads) k_mr_update(const __grid_constant__ 
         a.vpx[j] = a.vx[j];
         a.vx[j] = a.px[j] * ib;
     }
-    for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
+    for (int i = r0 + threadIdx.x; i < r1; i += NT) {
         const double w = (a.vy[i] - oldeps * a.d2y[i] - delta * a.d1y[i]) * ig;
         a.d2y[i] = a.d1y[i];
         a.d1y[i] = w;
         a.sy[i] += phi * w;
         a.vpy[i] = a.vy[i];
         a.vy[i] = a.py[i] * ib;
+    }
+}
+
+// One MINRES step per instance (one CTA per instance), after k_mr_op.
+__global__ void __launch_bounds__(kThreads) k_mr_update(const __grid_constant__ MrVecs a) {
+    __shared__ double red[kWarps];
+    __shared__ double bc[6];
+    const int k = blockIdx.x;
+    MrState* sp = a.st + k;
+    if (sp->done) return;
+    mr_update_step<kThreads>(a, k, sp, red, bc);
+}
+
+// Every MINRES step of one instance in one CTA, for reduced systems small
+// enough that one CTA forms p = K v in a few microseconds: the B pass (rows D
+// of the instance, giving the y-part) and the B^T pass (rows F, the x-part),
+// kMrLanes lanes per row summed by shuffles in a fixed order, then
+// mr_update_step; until the instance's state is done, which its step bound
+// guarantees.  Instances are independent, so CTAs never wait on one another.
+constexpr int kMrLanes = 2;
+constexpr int kMrSolveThreads = 512;  // a step's passes and sweeps over ~1,000 entries in one or two rounds
+constexpr long long kMrOneLaunchNnz = 1 << 16;  // B and B^T nonzeros of the widest instance
+bool mr_one_launch_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("GANIT_B200_MR_ONE_LAUNCH");
+        return v == nullptr || std::string(v) != "0";
+    }();
+    return on;
+}
+__device__ __forceinline__ void mr_rows(const CsrView<double>& B, int r0, int r1, const double* v, double* out) {
+    const int lane = threadIdx.x % kMrLanes, grp = threadIdx.x / kMrLanes;
+    constexpr int ngrp = kMrSolveThreads / kMrLanes;
+    for (int base = r0; base < r1; base += ngrp) {  // the same number of rounds for every thread
+        const int r = base + grp;
+        double t = 0.0;
+        if (r < r1) {
+            const int p1 = B.ptr[r + 1];
+#pragma unroll 4
+            for (int q = B.ptr[r] + lane; q < p1; q += kMrLanes) t += B.val[q] * v[B.idx[q]];
+        }
+#pragma unroll
+        for (int o = kMrLanes / 2; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o, kMrLanes);
+        if (r < r1 && lane == 0) out[r] = t;
+    }
+}
+__global__ void __launch_bounds__(kMrSolveThreads) k_mr_solve(const __grid_constant__ MrOpArgs a) {
+    __shared__ double red[kMrSolveThreads / 32];
+    __shared__ double bc[6];
+    const int k = blockIdx.x;
+    MrState* sp = a.v.st + k;
+    const int f0 = a.v.col_off[k], f1 = a.v.col_off[k + 1], d0 = a.v.row_off[k], d1 = a.v.row_off[k + 1];
+    while (*reinterpret_cast<volatile const int*>(&sp->done) == 0) {  // uniform: read after a barrier
+        mr_rows(a.A, d0, d1, a.v.vx, a.v.py);
+        mr_rows(a.AT, f0, f1, a.v.vy, a.v.px);
+        __syncthreads();
+        mr_update_step<kMrSolveThreads>(a.v, k, sp, red, bc);
+        __syncthreads();  // v and the state are written before the next step reads them
     }
 }
 
@@ -809,7 +880,16 @@ struct Diff {
         MrOpArgs oa{reduced_view(b_ptr, b_idx, b_val, b_s, nd), reduced_view(bt_ptr, bt_idx, bt_val, bt_s, nf), v};
         const int nb = oa.A.nb + oa.AT.nb;
         mr_graph.reset();  // it holds the previous system's schedules
-        if (host_loop_mode()) {  // the same steps from the host, one state read-back per chunk
+        // the whole solve in one launch, one CTA per instance, when every
+        // instance's B and B^T are small (GANIT_B200_MR_ONE_LAUNCH=0: never)
+        long long widest = 0;
+        for (int k = 0; k < p.count; ++k)
+            widest = std::max<long long>(widest, (b_ptr_h[mr_doff_h[k + 1]] - b_ptr_h[mr_doff_h[k]]) +
+                                                     (bt_ptr_h[mr_foff_h[k + 1]] - bt_ptr_h[mr_foff_h[k]]));
+        const bool one_launch = mr_one_launch_enabled() && widest <= kMrOneLaunchNnz;
+        if (one_launch) {
+            k_mr_solve<<<p.count, kMrSolveThreads, 0, s>>>(oa);
+        } else if (host_loop_mode()) {  // the same steps from the host, one state read-back per chunk
             for (;;) {
                 for (int c = 0; c < kMrChunk; ++c) {
                     if (nb) k_mr_op<<<nb, kThreads, smem, s>>>(oa);
@@ -870,7 +950,7 @@ struct Diff {
         GB_CUDA(cudaStreamSynchronize(s));
         long long steps = 0;
         for (int k = 0; k < p.count; ++k) steps = std::max<long long>(steps, mst_host[k].it);
-        launches += 1 + ((steps + kMrChunk - 1) / kMrChunk) * (2 * kMrChunk + 1);
+        launches += 1 + (one_launch ? 1 : ((steps + kMrChunk - 1) / kMrChunk) * (2 * kMrChunk + 1));
     }
 };
 
