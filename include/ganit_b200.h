@@ -458,7 +458,7 @@ int gb_strong_branch(const gb_lp* lp, const double* x, const double* y, int32_t 
  * (and implicit_max_iters > 0) and opt->tol below 4e-4, the solve goes in
  * rounds: first to 4e-4; every instance whose polished vertex certifies at
  * opt->tol keeps it; the rest continue, warm-started from their points, at a
- * tolerance ten times tighter per round, down to opt->tol, where the last
+ * tolerance four times tighter per round, down to opt->tol, where the last
  * round polishes as above (results[].iterations counts every round).
  * Backward: given dL/dx* and dL/dy*, exact reverse mode through the K tail
  * iterations (each R-segment recomputed from its checkpoint; projections,
