@@ -1185,6 +1185,10 @@ void diff_forward(Diff& D, const gb_options* opt, gb_result* res, double* x_out,
     // step bound, and a forward with no polishing keeps one cold solve)
     o.tol = D.polish && D.mr_max > 0 && target < kPolishFirstTol ? kPolishFirstTol : target;
     std::vector<int> todo(K, 1), kept(K, 0);
+    // the first round starts cold, whatever an interrupted forward left behind
+    P.x_start.release();
+    P.y_start.release();
+    P.w_start.release();
     std::vector<long long> its(K, 0);
     long long launches = 0;
     bool any_kept = false;
