@@ -411,15 +411,16 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     const int lg_a = lanes_lg(P->A.nnz, m), lg_at = lanes_lg(P->A.nnz, n);
     for (int it = 0; it < passes; ++it) {
         const int mode = it < opt->ruiz_iters ? 0 : 1;
-        k_row_norm_factor<<<gw, kThreads, 0, s>>>(m, P->A.ptr.get(), nullptr, P->A.val64.get(), mode, rs.get(),
-                                                  mode == 0 ? lg_a : 5);
-        k_row_norm_factor<<<gw, kThreads, 0, s>>>(n, P->AT.ptr.get(), P->perm.get(), P->A.val64.get(), mode, cs.get(),
-                                                  mode == 0 ? lg_at : 5);
-        if (P->A.nnz)
-            k_apply_scaling<<<ge, kThreads, 0, s>>>(static_cast<int>(P->A.nnz), P->row_of.get(), P->A.idx.get(),
-                                                    rs.get(), cs.get(), P->A.val64.get());
-        k_mul_into<<<elem_grid(m, P->sms), kThreads, 0, s>>>(m, rs.get(), P->R.get());
-        k_mul_into<<<elem_grid(n, P->sms), kThreads, 0, s>>>(n, cs.get(), P->C.get());
+        launch_pdl(k_row_norm_factor, gw, kThreads, 0, s, m, static_cast<const int*>(P->A.ptr.get()),
+                   static_cast<const int*>(nullptr), static_cast<const double*>(P->A.val64.get()), mode, rs.get(),
+                   mode == 0 ? lg_a : 5);
+        launch_pdl(k_row_norm_factor, gw, kThreads, 0, s, n, static_cast<const int*>(P->AT.ptr.get()),
+                   static_cast<const int*>(P->perm.get()), static_cast<const double*>(P->A.val64.get()), mode, cs.get(),
+                   mode == 0 ? lg_at : 5);
+        launch_pdl(k_apply_scaling, std::max(ge, elem_grid(std::max(m, n), P->sms)), kThreads, 0, s,
+                   static_cast<int>(P->A.nnz), static_cast<const int*>(P->row_of.get()),
+                   static_cast<const int*>(P->A.idx.get()), static_cast<const double*>(rs.get()),
+                   static_cast<const double*>(cs.get()), P->A.val64.get(), m, P->R.get(), n, P->C.get());
     }
     if (P->A.nnz)
         k_gather_transpose<<<ge, kThreads, 0, s>>>(static_cast<int>(P->A.nnz), P->perm.get(), P->row_of.get(),

@@ -121,6 +121,7 @@ static __global__ void k_gather_transpose(int nnz, const int* __restrict__ perm,
 // shuffles always see the whole warp.
 static __global__ void k_row_norm_factor(int rows, const int* __restrict__ ptr, const int* __restrict__ perm,
                                   const double* __restrict__ val, int mode, double* __restrict__ fac, int lg) {
+    pdl_enter();
     const int G = 1 << lg, rpw = 32 >> lg;  // lanes per row, rows per warp and round
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane32 = threadIdx.x & 31;
     const int lane = lane32 & (G - 1);
@@ -143,13 +144,16 @@ static __global__ void k_row_norm_factor(int rows, const int* __restrict__ ptr, 
 }
 
 // apply (scaling.cpp:27-33): val *= rs[row] * cs[col]
+// One Ruiz / Pock-Chambolle pass applied (scaling.cpp:27-33): a_ij *= rs_i cs_j,
+// R *= rs, C *= cs, in one launch.
 static __global__ void k_apply_scaling(int nnz, const int* __restrict__ row_of, const int* __restrict__ idx,
-                                const double* __restrict__ rs, const double* __restrict__ cs, double* __restrict__ val) {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += gridDim.x * blockDim.x)
-        val[p] *= rs[row_of[p]] * cs[idx[p]];
-}
-static __global__ void k_mul_into(int n, const double* __restrict__ f, double* __restrict__ v) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] *= f[i];
+                                const double* __restrict__ rs, const double* __restrict__ cs, double* __restrict__ val,
+                                int m, double* __restrict__ R, int n, double* __restrict__ C) {
+    pdl_enter();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    for (int p = t; p < nnz; p += stride) val[p] *= rs[row_of[p]] * cs[idx[p]];
+    for (int i = t; i < m; i += stride) R[i] *= rs[i];
+    for (int j = t; j < n; j += stride) C[j] *= cs[j];
 }
 static __global__ void k_fill(int n, double a, double* __restrict__ v) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = a;
