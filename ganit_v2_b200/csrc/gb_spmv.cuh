@@ -70,15 +70,29 @@ struct Schedule {
 
 // Appends the row-start bitmap of a STREAM block to s.bits and records its
 // offset in b.slot_base (a field CHUNK blocks use for their slots).
+// Row starts increase along the block, so each word is gathered in a
+// register and stored once.
 inline void add_stream_bits(Schedule& s, const int* ptr, RowBlock& b) {
     const int a = b.p0 & 3, nq = ((b.p1 + 3) >> 2) - (b.p0 >> 2);
     const size_t off = s.bits.size();
     s.bits.resize(off + (4 * static_cast<size_t>(nq) + 31) / 32, 0u);
-    for (int i = b.r0; i < b.r1; ++i)
-        if (ptr[i + 1] > ptr[i]) {
-            const int t = ptr[i] - b.p0 + a;
-            s.bits[off + (t >> 5)] |= 1u << (t & 31);
+    unsigned* w = s.bits.data() + off;
+    const int base = a - b.p0;
+    int cur = -1;
+    unsigned acc = 0u;
+    for (int i = b.r0; i < b.r1; ++i) {
+        const int p = ptr[i];
+        if (ptr[i + 1] > p) {
+            const int t = p + base, k = t >> 5;
+            if (k != cur) {
+                if (cur >= 0) w[cur] |= acc;
+                cur = k;
+                acc = 0u;
+            }
+            acc |= 1u << (t & 31);
         }
+    }
+    if (cur >= 0) w[cur] |= acc;
     b.slot_base = static_cast<int>(off);
 }
 
@@ -157,6 +171,7 @@ inline Schedule build_schedule(const int* ptr, int rows, const int* seg_off = nu
                                int block_nnz = kBlockNnz, int max_rows = kThreads) {
     Schedule s;
     s.seg_block.assign(nseg + 1, 0);
+    s.bits.reserve(static_cast<size_t>(ptr[seg_off ? seg_off[nseg] : rows]) / 8 + 64);  // ~4 words per 128 nonzeros
     for (int k = 0; k < nseg; ++k) {
         s.seg_block[k] = static_cast<int>(s.blocks.size());
         const int r0 = seg_off ? seg_off[k] : 0, r1 = seg_off ? seg_off[k + 1] : rows;
@@ -175,6 +190,7 @@ inline Schedule build_schedule(const int* ptr, const int* seg_off, int nseg, con
                                const int* max_rows) {
     Schedule s;
     s.seg_block.assign(nseg + 1, 0);
+    s.bits.reserve(static_cast<size_t>(ptr[seg_off[nseg]]) / 8 + 64);
     for (int k = 0; k < nseg; ++k) {
         s.seg_block[k] = static_cast<int>(s.blocks.size());
         schedule_rows(ptr, seg_off[k], seg_off[k + 1], block_nnz[k], max_rows[k], &s.nslots, &s.ncounters, k,
