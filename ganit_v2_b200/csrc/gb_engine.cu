@@ -115,26 +115,33 @@ struct TransposeScratch {
     DevBuf<int> cnt, tile_sum;
     SortScratch sort;
 };
+// With host_ptr, t_ptr is also copied to that pageable host array as soon as
+// it is formed: the copy returns then, and the sort and gather are enqueued
+// after it, so the caller works on t_ptr while they run.
 void transpose_csr(int rows, int cols, int nnz, const int* ptr, const int* idx, const double* val, int* row_of,
-                   int* perm, int* t_ptr, int* t_idx, double* t_val, int sms, TransposeScratch& w, cudaStream_t s) {
+                   int* perm, int* t_ptr, int* t_idx, double* t_val, int sms, TransposeScratch& w, cudaStream_t s,
+                   int* host_ptr = nullptr) {
     const int g = elem_grid(std::max<long long>(nnz, static_cast<long long>(rows) * 32), sms);
     if (rows) k_row_of<<<g, kThreads, 0, s>>>(rows, ptr, row_of);
     w.cnt.reset(cols + 1);
     w.tile_sum.reset(scan_tiles(cols + 1));
     GB_CUDA(cudaMemsetAsync(w.cnt.get(), 0, sizeof(int) * (cols + 1), s));
+    if (nnz) k_count_cols<<<elem_grid(nnz, sms), kThreads, 0, s>>>(nnz, idx, w.cnt.get());
+    exclusive_scan(w.cnt.get(), t_ptr, cols + 1, w.tile_sum.get(), s);
+    if (host_ptr)
+        GB_CUDA(cudaMemcpyAsync(host_ptr, t_ptr, sizeof(int) * (cols + 1), cudaMemcpyDeviceToHost, s));
     if (nnz) {
-        k_count_cols<<<elem_grid(nnz, sms), kThreads, 0, s>>>(nnz, idx, w.cnt.get());
         int bits = 0;  // column keys lie in [0, 2^bits)
         while ((1LL << bits) < cols) ++bits;
         stable_sort_index(idx, nnz, bits, perm, sms, w.sort, s);
         k_gather_transpose<<<elem_grid(nnz, sms), kThreads, 0, s>>>(nnz, perm, row_of, val, t_idx, t_val);
     }
-    exclusive_scan(w.cnt.get(), t_ptr, cols + 1, w.tile_sum.get(), s);
 }
 
 // A^T of a problem: its structure now, its values after the scaling
-// (k_gather_transpose through perm again).
-void device_transpose(Problem& P, cudaStream_t s) {
+// (k_gather_transpose through perm again).  Returns with A^T's row pointers
+// on the host while the sort may still run; `w` must outlive it.
+void device_transpose(Problem& P, TransposeScratch& w, cudaStream_t s) {
     const int nnz = static_cast<int>(P.A.nnz), n = P.n, m = P.m;
     P.AT.rows = n;
     P.AT.cols = m;
@@ -144,12 +151,10 @@ void device_transpose(Problem& P, cudaStream_t s) {
     P.AT.ptr.reset(n + 1);
     P.AT.idx.reset(padded_nnz(nnz));
     P.AT.val64.reset(padded_nnz(nnz));
-    TransposeScratch w;  // released after the synchronisation below
-    transpose_csr(m, n, nnz, P.A.ptr.get(), P.A.idx.get(), nullptr, P.row_of.get(), P.perm.get(), P.AT.ptr.get(),
-                  P.AT.idx.get(), nullptr, P.sms, w, s);
     P.AT.host_ptr.resize(n + 1);
-    GB_CUDA(cudaMemcpyAsync(P.AT.host_ptr.data(), P.AT.ptr.get(), sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
-    GB_CUDA(cudaStreamSynchronize(s));
+    // (a pageable destination: the copy returns once done, before the sort)
+    transpose_csr(m, n, nnz, P.A.ptr.get(), P.A.idx.get(), nullptr, P.row_of.get(), P.perm.get(), P.AT.ptr.get(),
+                  P.AT.idx.get(), nullptr, P.sms, w, s, P.AT.host_ptr.data());
 }
 
 // Per-instance fixed-order reduction into scal[k][slot]: rows (m) or columns (n).
@@ -390,7 +395,8 @@ Problem* create_problem(int count, const gb_lp* lps, const gb_options* opt) {
     }
     P->A.sched.upload(build_schedule(P->A.host_ptr.data(), m, P->row_off.data(), count), 3, s);
     tr.mark("allocs+A schedule");
-    device_transpose(*P, s);
+    TransposeScratch tw;  // lives until the set-up's final synchronisation
+    device_transpose(*P, tw, s);
     tr.mark("transpose");
 
     // Ruiz equilibration + Pock-Chambolle (scaling.cpp:47-72); row and column
